@@ -1,0 +1,132 @@
+/*
+ * sbdgpu.h -- C ABI of the B200 (sm_100a) tensor-product-basis Davidson path.
+ *
+ * This is the boundary the header-only C++ host library (sbd::tpb::diag, the
+ * drop-in for the reference entry point chemistry/tpb/sbdiag.h:102-113) calls.
+ * Plain C types only: pointers, sizes, status codes.  Nothing throws across it.
+ *
+ * Conventions (all shared with the reference):
+ *  - norb <= 64; a string is a uint64 with orbital i at bit i (the reference
+ *    packs bit_length bits per size_t word, framework/bit_manipulation.h:158-172;
+ *    the host side re-packs).  alpha/beta strings are given in the order the
+ *    reference holds them (sorted ascending unless shuffled, main.cc:122-132).
+ *  - Wavefunction and sigma vectors are row-major [na][nb]: index ia*nb + ib
+ *    (chemistry/tpb/qcham.h:359, mult.h:503), in the reference's interleaved
+ *    spin-orbital sign convention (chemistry/basic/determinants.h:98-119).
+ *  - One-body integrals h1[p*norb+q] (spatial); two-body integrals in the
+ *    reference's 8-fold packed store (chemistry/basic/integrals.h:34-43):
+ *    ij = max(i,j)(max(i,j)+1)/2 + min(i,j), element at a(a+1)/2+b with
+ *    a = max(ij,kl), b = min(ij,kl); length P(P+1)/2, P = norb(norb+1)/2.
+ *  - Status: 0 = success; nonzero = error, text from sbdgpu_last_error().
+ *  - Host pointers are synchronous in/out and stay owned by the caller.  Device
+ *    memory, the stream and kernels belong to the context.  A context is not
+ *    thread-safe: use one per host thread.
+ */
+#ifndef SBDGPU_H
+#define SBDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sbdgpu_ctx sbdgpu_ctx;
+
+#define SBDGPU_OK 0
+#define SBDGPU_ERR_ARG 1
+#define SBDGPU_ERR_CUDA 2
+#define SBDGPU_ERR_ALLOC 3
+#define SBDGPU_ERR_LIMIT 4
+#define SBDGPU_ERR_STATE 5
+
+/* Arithmetic of a sigma build. */
+#define SBDGPU_FP64 0 /* plain path: every product and sum in FP64 */
+
+/* Davidson options: the reference SBD fields that steer the solver
+ * (chemistry/tpb/sbdiag.h:12-30). */
+typedef struct sbdgpu_opts {
+  int max_it;       /* SBD::max_it (--iteration), restarts */
+  int max_nb;       /* SBD::max_nb (--block), Krylov block <= 32 */
+  double eps;       /* SBD::eps (--tolerance), residual-norm target */
+  double max_time;  /* SBD::max_time, wall-time budget in seconds */
+  int precision;    /* SBDGPU_FP64 */
+  int verbose;      /* 1: print the reference's "Davidson iteration" lines */
+} sbdgpu_opts;
+
+/* Create a context on CUDA device `device` for one alpha x beta product basis
+ * and Hamiltonian.  Replaces the set-up half of sbd::tpb::diag
+ * (chemistry/tpb/sbdiag.h:143-166: SetupIntegrals, TaskCommunicator,
+ * MakeHelpers/RemakeHelpers).  Copies all inputs. */
+int sbdgpu_create(sbdgpu_ctx** out, int norb, size_t na, size_t nb, const uint64_t* astr,
+                  const uint64_t* bstr, double ecore, const double* h1, const double* eri_packed,
+                  int device);
+
+/* Build the excitation tables on the GPU.  Replaces GenerateExcitation /
+ * MakeSmartHelper (chemistry/tpb/helper.h:132-182, 352-422).  Called
+ * implicitly by every routine that needs the tables. */
+int sbdgpu_build_tables(sbdgpu_ctx* ctx);
+
+/* Table sizes for spin (0 alpha, 1 beta): total singles and doubles entries. */
+int sbdgpu_table_sizes(sbdgpu_ctx* ctx, int spin, uint64_t* n_singles, uint64_t* n_doubles);
+
+/* Copy one spin's tables to the host in the reference helper layout: for bra
+ * string i, kets single_idx[single_off[i] .. single_off[i+1]) ascending
+ * (SinglesFromAlphaSM / SinglesFromAlphaLen, helper.h:352-422); same for
+ * doubles.  Offsets have n+1 entries. */
+int sbdgpu_get_tables(sbdgpu_ctx* ctx, int spin, uint64_t* single_off, uint64_t* single_idx,
+                      uint64_t* double_off, uint64_t* double_idx);
+
+/* Diagonal H_ii for every determinant (row-major).  Replaces
+ * makeQChamDiagTerms (chemistry/tpb/qcham.h:314-366). */
+int sbdgpu_diag(sbdgpu_ctx* ctx, double* hii);
+
+/* sigma = H*C with host vectors (na*nb doubles each).  Replaces the direct
+ * mult (chemistry/tpb/mult.h:387-648); unlike mult, sigma is overwritten
+ * rather than accumulated into. */
+int sbdgpu_sigma(sbdgpu_ctx* ctx, const double* C, double* sigma, int precision);
+
+/* sigma = H*C with device vectors (na*nb doubles each, on this context's
+ * device).  The work is issued on the context's stream; the call returns
+ * after it completes. */
+int sbdgpu_sigma_device(sbdgpu_ctx* ctx, const double* dC, double* dsigma, int precision);
+
+/* Restarted Davidson for the lowest root, the reference algorithm of
+ * chemistry/tpb/davidson.h:661-923 (block <= max_nb, collapse restart,
+ * diagonal preconditioner with eps_reg = 1e-12, modified Gram-Schmidt,
+ * wall-time budget), followed by E = <W|HW> from one more sigma
+ * (sbdiag.h:239-262).
+ *   W         in: initial vector (na*nb, normalised or not); out: Ritz vector
+ *   energy    out: <W|HW>
+ *   trace_e / trace_tol  optional (may be NULL): lowest Ritz value and residual
+ *             norm per step, up to max_trace entries
+ *   n_steps   out: steps taken (sigma builds inside the loop) */
+int sbdgpu_davidson(sbdgpu_ctx* ctx, const sbdgpu_opts* opts, double* W, double* energy,
+                    double* trace_e, double* trace_tol, int max_trace, int* n_steps);
+
+/* One- and two-particle RDMs of W in the reference layout
+ * one[s*L*L + i + L*j], two[(s + 2t)*L^4 + i + L*j + L^2*k + L^3*l]
+ * (chemistry/tpb/correlation.h:194-443, docs/user-guide.md:138-139). */
+int sbdgpu_rdm(sbdgpu_ctx* ctx, const double* W, double* one, double* two);
+
+/* Orbital occupations density[2p] (alpha), density[2p+1] (beta).  Replaces
+ * OccupationDensity (chemistry/tpb/occupation.h:10-95). */
+int sbdgpu_occupation(sbdgpu_ctx* ctx, const double* W, double* density);
+
+/* Per-alpha-string weights D[ia] = sum_ib W[ia,ib]^2, the input of the
+ * carry-over selection (DiagonalReducedDensityMatrix, chemistry/tpb/rdmat.h:11-58). */
+int sbdgpu_alpha_weights(sbdgpu_ctx* ctx, const double* W, double* D);
+
+/* Device time in milliseconds of the kernels of the last sigma build, split
+ * as [diagonal+alpha same-spin, beta same-spin incl. transposes, alpha-beta]. */
+int sbdgpu_last_sigma_ms(sbdgpu_ctx* ctx, float* ms3);
+
+const char* sbdgpu_last_error(sbdgpu_ctx* ctx);
+void sbdgpu_destroy(sbdgpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SBDGPU_H */

@@ -1,0 +1,177 @@
+"""sbd_b200: the tensor-product-basis Davidson path of r-ccs-cms/sbd on B200.
+
+Python binding (ctypes) of the C ABI declared in include/sbdgpu.h, implemented
+by the in-tree library sbd_b200/libsbdgpu.so.  There is no CPU fallback: if the
+library is missing, or no CUDA device is present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsbdgpu.so")
+
+FP64 = 0
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+EXPORTS = [
+    "sbdgpu_create", "sbdgpu_build_tables", "sbdgpu_table_sizes", "sbdgpu_get_tables", "sbdgpu_diag",
+    "sbdgpu_sigma", "sbdgpu_sigma_device", "sbdgpu_davidson", "sbdgpu_rdm", "sbdgpu_occupation",
+    "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
+]
+
+
+class SbdGpuError(RuntimeError):
+    pass
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("max_it", ctypes.c_int), ("max_nb", ctypes.c_int), ("eps", ctypes.c_double),
+                ("max_time", ctypes.c_double), ("precision", ctypes.c_int), ("verbose", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libsbdgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SbdGpuError(f"{LIB_PATH} is missing: build it with sbd_b200.build.build_lib()")
+        L = ctypes.CDLL(LIB_PATH)
+        L.sbdgpu_create.restype = ctypes.c_int
+        L.sbdgpu_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_size_t, ctypes.c_size_t, _u64p,
+                                    _u64p, ctypes.c_double, _dp, _dp, ctypes.c_int]
+        L.sbdgpu_build_tables.argtypes = [_vp]
+        L.sbdgpu_table_sizes.argtypes = [_vp, ctypes.c_int, _u64p, _u64p]
+        L.sbdgpu_get_tables.argtypes = [_vp, ctypes.c_int, _u64p, _u64p, _u64p, _u64p]
+        L.sbdgpu_diag.argtypes = [_vp, _dp]
+        L.sbdgpu_sigma.argtypes = [_vp, _dp, _dp, ctypes.c_int]
+        L.sbdgpu_sigma_device.argtypes = [_vp, _vp, _vp, ctypes.c_int]
+        L.sbdgpu_davidson.argtypes = [_vp, ctypes.POINTER(Opts), _dp, _dp, _dp, _dp, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
+        L.sbdgpu_occupation.argtypes = [_vp, _dp, _dp]
+        L.sbdgpu_alpha_weights.argtypes = [_vp, _dp, _dp]
+        L.sbdgpu_last_sigma_ms.argtypes = [_vp, ctypes.POINTER(ctypes.c_float)]
+        L.sbdgpu_last_error.restype = ctypes.c_char_p
+        L.sbdgpu_last_error.argtypes = [_vp]
+        L.sbdgpu_destroy.argtypes = [_vp]
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+class Context:
+    """One alpha x beta product basis and Hamiltonian on one GPU."""
+
+    def __init__(self, norb: int, astr, bstr, ecore: float, h1: np.ndarray, eri_packed: np.ndarray,
+                 device: int = 0):
+        self.norb = int(norb)
+        self.astr = np.ascontiguousarray(astr, dtype=np.uint64)
+        self.bstr = np.ascontiguousarray(bstr, dtype=np.uint64)
+        self.na, self.nb = len(self.astr), len(self.bstr)
+        self.n = self.na * self.nb
+        h = np.ascontiguousarray(h1, dtype=np.float64)
+        e = np.ascontiguousarray(eri_packed, dtype=np.float64)
+        self._h = _vp()
+        rc = lib().sbdgpu_create(ctypes.byref(self._h), self.norb, self.na, self.nb, _p(self.astr, _u64p),
+                                 _p(self.bstr, _u64p), float(ecore), _p(h, _dp), _p(e, _dp), int(device))
+        if rc != 0:
+            raise SbdGpuError(f"sbdgpu_create failed with status {rc}")
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = lib().sbdgpu_last_error(self._h)
+            raise SbdGpuError(f"status {rc}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sbdgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def tables(self, spin: int):
+        ns, nd = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        self._check(lib().sbdgpu_table_sizes(self._h, spin, ctypes.byref(ns), ctypes.byref(nd)))
+        n = self.na if spin == 0 else self.nb
+        so = np.zeros(n + 1, np.uint64)
+        do = np.zeros(n + 1, np.uint64)
+        si = np.zeros(max(ns.value, 1), np.uint64)
+        di = np.zeros(max(nd.value, 1), np.uint64)
+        self._check(lib().sbdgpu_get_tables(self._h, spin, _p(so, _u64p), _p(si, _u64p), _p(do, _u64p),
+                                            _p(di, _u64p)))
+        return so, si[:ns.value], do, di[:nd.value]
+
+    def hii(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        self._check(lib().sbdgpu_diag(self._h, _p(out, _dp)))
+        return out
+
+    def sigma(self, C: np.ndarray, precision: int = FP64) -> np.ndarray:
+        C = np.ascontiguousarray(C, dtype=np.float64).ravel()
+        out = np.zeros(self.n)
+        self._check(lib().sbdgpu_sigma(self._h, _p(C, _dp), _p(out, _dp), precision))
+        return out
+
+    def sigma_device(self, dC_ptr: int, dS_ptr: int, precision: int = FP64) -> None:
+        self._check(lib().sbdgpu_sigma_device(self._h, _vp(dC_ptr), _vp(dS_ptr), precision))
+
+    def last_sigma_ms(self):
+        a = (ctypes.c_float * 3)()
+        self._check(lib().sbdgpu_last_sigma_ms(self._h, a))
+        return [float(x) for x in a]
+
+    def davidson(self, W0: np.ndarray, max_it: int, max_nb: int, eps: float, max_time: float = 86400.0,
+                 precision: int = FP64, verbose: int = 0, max_trace: int = 100000):
+        W = np.ascontiguousarray(W0, dtype=np.float64).ravel().copy()
+        o = Opts(max_it, max_nb, eps, max_time, precision, verbose)
+        e = ctypes.c_double(0.0)
+        te = np.zeros(max_trace)
+        tt = np.zeros(max_trace)
+        ns = ctypes.c_int(0)
+        self._check(lib().sbdgpu_davidson(self._h, ctypes.byref(o), _p(W, _dp), ctypes.byref(e), _p(te, _dp),
+                                          _p(tt, _dp), max_trace, ctypes.byref(ns)))
+        k = min(ns.value, max_trace)
+        return e.value, W, te[:k], tt[:k]
+
+    def rdm(self, W: np.ndarray):
+        W = np.ascontiguousarray(W, dtype=np.float64).ravel()
+        L = self.norb
+        one = np.zeros(2 * L * L)
+        two = np.zeros(4 * L ** 4)
+        self._check(lib().sbdgpu_rdm(self._h, _p(W, _dp), _p(one, _dp), _p(two, _dp)))
+        return one, two
+
+    def occupation(self, W: np.ndarray) -> np.ndarray:
+        W = np.ascontiguousarray(W, dtype=np.float64).ravel()
+        d = np.zeros(2 * self.norb)
+        self._check(lib().sbdgpu_occupation(self._h, _p(W, _dp), _p(d, _dp)))
+        return d
+
+    def alpha_weights(self, W: np.ndarray) -> np.ndarray:
+        W = np.ascontiguousarray(W, dtype=np.float64).ravel()
+        d = np.zeros(self.na)
+        self._check(lib().sbdgpu_alpha_weights(self._h, _p(W, _dp), _p(d, _dp)))
+        return d
+
+
+def context_from_integrals(ints, astr, bstr, device: int = 0) -> Context:
+    """Context from an object with .norb, .ecore, .h [L,L] and .eri [L,L,L,L]."""
+    from .synth import pack_eri
+    return Context(ints.norb, astr, bstr, ints.ecore, ints.h, pack_eri(ints.eri), device)

@@ -1,0 +1,408 @@
+// C ABI (include/sbdgpu.h): context life cycle, host/device transfers and the
+// Davidson driver.  No exception crosses the ABI; errors become status codes
+// with a message kept in the context.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include <new>
+
+#include "internal.cuh"
+
+using sbdgpu::Error;
+
+namespace sbdgpu {
+
+void* dev_alloc(size_t bytes) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes ? bytes : 8);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error{SBDGPU_ERR_ALLOC, "device allocation of " + std::to_string(bytes) + " bytes failed: " +
+                                      cudaGetErrorString(e)};
+  }
+  return p;
+}
+
+void ensure_scratch(sbdgpu_ctx* c) {
+  if (!c->red) c->red = (double*)dev_alloc(sizeof(double) * 1024);
+  if (!c->ct) c->ct = (double*)dev_alloc(sizeof(double) * c->N);
+  if (!c->st) c->st = (double*)dev_alloc(sizeof(double) * c->N);
+}
+
+void ensure_io(sbdgpu_ctx* c) {
+  if (!c->io_a) c->io_a = (double*)dev_alloc(sizeof(double) * c->N);
+  if (!c->io_b) c->io_b = (double*)dev_alloc(sizeof(double) * c->N);
+}
+
+// Cyclic Jacobi eigen-solver for the small projected matrix (the reference
+// solves the same problem with LAPACK dsyev, framework/hp_numeric.h:500-517).
+// A: n x n column-major, leading dimension lda; on return A holds the
+// eigenvectors (columns) in ascending eigenvalue order, w the eigenvalues.
+void jacobi_eig(int n, double* A, int lda, double* w) {
+  std::vector<double> M(n * n), V(n * n, 0.0);
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < n; i++) M[i + j * n] = A[i + j * lda];
+  for (int i = 0; i < n; i++) V[i + i * n] = 1.0;
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0.0;
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < j; i++) off += M[i + j * n] * M[i + j * n];
+    if (off < 1e-300) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        double apq = M[p + q * n];
+        if (std::fabs(apq) < 1e-300) continue;
+        double theta = 0.5 * (M[q + q * n] - M[p + p * n]) / apq;
+        double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < n; k++) {
+          double a = M[k + p * n], b = M[k + q * n];
+          M[k + p * n] = cs * a - sn * b;
+          M[k + q * n] = sn * a + cs * b;
+        }
+        for (int k = 0; k < n; k++) {
+          double a = M[p + k * n], b = M[q + k * n];
+          M[p + k * n] = cs * a - sn * b;
+          M[q + k * n] = sn * a + cs * b;
+        }
+        for (int k = 0; k < n; k++) {
+          double a = V[k + p * n], b = V[k + q * n];
+          V[k + p * n] = cs * a - sn * b;
+          V[k + q * n] = sn * a + cs * b;
+        }
+      }
+  }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; i++) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return M[a + a * n] < M[b + b * n]; });
+  for (int k = 0; k < n; k++) {
+    int s = order[k];
+    w[k] = M[s + s * n];
+    for (int i = 0; i < n; i++) A[i + k * lda] = V[i + s * n];
+  }
+}
+
+}  // namespace sbdgpu
+
+namespace {
+
+template <class F>
+int guarded(sbdgpu_ctx* c, F&& f) {
+  if (!c) return SBDGPU_ERR_ARG;
+  try {
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) throw Error{SBDGPU_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e)};
+    f();
+    c->err.clear();
+    return SBDGPU_OK;
+  } catch (const Error& e) {
+    c->err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    c->err = "host allocation failed";
+    return SBDGPU_ERR_ALLOC;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return SBDGPU_ERR_STATE;
+  }
+}
+
+using sbdgpu::ensure_io;
+
+void check_precision(int precision) {
+  if (precision != SBDGPU_FP64) throw Error{SBDGPU_ERR_ARG, "unsupported precision " + std::to_string(precision)};
+}
+
+void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS) {
+  // dC, dS in the reference (interleaved) sign convention
+  ensure_io(c);
+  SBD_CUDA(cudaMemcpyAsync(c->io_a, dC, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+  sbdgpu::build_tables(c);
+  sbdgpu::apply_phase(c, c->io_a);
+  sbdgpu::sigma_fp64(c, c->io_a, dS);
+  sbdgpu::apply_phase(c, dS);
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; k++) SBD_CUDA(cudaEventElapsedTime(&c->last_ms[k], c->ev[k], c->ev[k + 1]));
+}
+
+}  // namespace
+
+extern "C" {
+
+int sbdgpu_create(sbdgpu_ctx** out, int norb, size_t na, size_t nb, const uint64_t* astr, const uint64_t* bstr,
+                  double ecore, const double* h1, const double* eri_packed, int device) {
+  if (!out) return SBDGPU_ERR_ARG;
+  *out = nullptr;
+  if (norb < 1 || norb > 64 || na == 0 || nb == 0 || !astr || !bstr || !h1 || !eri_packed) return SBDGPU_ERR_ARG;
+  for (size_t i = 0; i < na; i++)
+    if (norb < 64 && (astr[i] >> norb)) return SBDGPU_ERR_ARG;
+  for (size_t i = 0; i < nb; i++)
+    if (norb < 64 && (bstr[i] >> norb)) return SBDGPU_ERR_ARG;
+  if (na > (size_t)INT32_MAX || nb > (size_t)INT32_MAX) return SBDGPU_ERR_LIMIT;
+  sbdgpu_ctx* c = new (std::nothrow) sbdgpu_ctx();
+  if (!c) return SBDGPU_ERR_ALLOC;
+  c->device = device;
+  int rc = guarded(c, [&] {
+    c->L = norb;
+    c->P = norb * (norb + 1) / 2;
+    c->na = na;
+    c->nb = nb;
+    c->N = na * nb;
+    c->ecore = ecore;
+    c->h_astr.assign(astr, astr + na);
+    c->h_bstr.assign(bstr, bstr + nb);
+    c->h_h1.assign(h1, h1 + (size_t)norb * norb);
+    size_t P = c->P;
+    c->h_vf.resize(P * P);
+    for (size_t i = 0; i < P; i++)
+      for (size_t j = 0; j < P; j++) {
+        size_t a = std::max(i, j), b = std::min(i, j);
+        c->h_vf[i * P + j] = eri_packed[a * (a + 1) / 2 + b];
+      }
+    SBD_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 4; k++) SBD_CUDA(cudaEventCreate(&c->ev[k]));
+    c->astr = (uint64_t*)sbdgpu::dev_alloc(sizeof(uint64_t) * na);
+    c->bstr = (uint64_t*)sbdgpu::dev_alloc(sizeof(uint64_t) * nb);
+    c->h1 = (double*)sbdgpu::dev_alloc(sizeof(double) * norb * norb);
+    c->vf = (double*)sbdgpu::dev_alloc(sizeof(double) * P * P);
+    SBD_CUDA(cudaMemcpyAsync(c->astr, astr, sizeof(uint64_t) * na, cudaMemcpyHostToDevice, c->stream));
+    SBD_CUDA(cudaMemcpyAsync(c->bstr, bstr, sizeof(uint64_t) * nb, cudaMemcpyHostToDevice, c->stream));
+    SBD_CUDA(cudaMemcpyAsync(c->h1, h1, sizeof(double) * norb * norb, cudaMemcpyHostToDevice, c->stream));
+    SBD_CUDA(cudaMemcpyAsync(c->vf, c->h_vf.data(), sizeof(double) * P * P, cudaMemcpyHostToDevice, c->stream));
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+  });
+  if (rc != SBDGPU_OK) {
+    std::fprintf(stderr, "sbdgpu_create: %s\n", c->err.c_str());
+    sbdgpu_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return SBDGPU_OK;
+}
+
+int sbdgpu_build_tables(sbdgpu_ctx* c) {
+  return guarded(c, [&] { sbdgpu::build_tables(c); });
+}
+
+int sbdgpu_table_sizes(sbdgpu_ctx* c, int spin, uint64_t* ns, uint64_t* nd) {
+  return guarded(c, [&] {
+    if (spin < 0 || spin > 1) throw Error{SBDGPU_ERR_ARG, "spin must be 0 or 1"};
+    sbdgpu::build_tables(c);
+    if (ns) *ns = c->tab[spin].ns;
+    if (nd) *nd = c->tab[spin].nd;
+  });
+}
+
+int sbdgpu_get_tables(sbdgpu_ctx* c, int spin, uint64_t* s_off, uint64_t* s_idx, uint64_t* d_off, uint64_t* d_idx) {
+  return guarded(c, [&] {
+    if (spin < 0 || spin > 1) throw Error{SBDGPU_ERR_ARG, "spin must be 0 or 1"};
+    sbdgpu::build_tables(c);
+    const sbdgpu::SpinTables& t = c->tab[spin];
+    if (s_off)
+      for (size_t i = 0; i <= t.n; i++) s_off[i] = (uint64_t)t.h_s_off[i];
+    if (d_off)
+      for (size_t i = 0; i <= t.n; i++) d_off[i] = (uint64_t)t.h_d_off[i];
+    std::vector<int32_t> tmp;
+    if (s_idx && t.ns) {
+      tmp.resize(t.ns);
+      SBD_CUDA(cudaMemcpy(tmp.data(), t.s_idx, sizeof(int32_t) * t.ns, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < t.ns; i++) s_idx[i] = (uint64_t)tmp[i];
+    }
+    if (d_idx && t.nd) {
+      tmp.resize(t.nd);
+      SBD_CUDA(cudaMemcpy(tmp.data(), t.d_idx, sizeof(int32_t) * t.nd, cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < t.nd; i++) d_idx[i] = (uint64_t)tmp[i];
+    }
+  });
+}
+
+int sbdgpu_diag(sbdgpu_ctx* c, double* hii) {
+  return guarded(c, [&] {
+    if (!hii) throw Error{SBDGPU_ERR_ARG, "null output"};
+    sbdgpu::build_tables(c);
+    sbdgpu::compute_hii(c);
+    SBD_CUDA(cudaMemcpyAsync(hii, c->hii, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int sbdgpu_sigma(sbdgpu_ctx* c, const double* C, double* S, int precision) {
+  return guarded(c, [&] {
+    if (!C || !S) throw Error{SBDGPU_ERR_ARG, "null vector"};
+    check_precision(precision);
+    ensure_io(c);
+    SBD_CUDA(cudaMemcpyAsync(c->io_b, C, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    // sigma_ref_convention stages the input in io_a, so io_b can take the result
+    sigma_ref_convention(c, c->io_b, c->io_b);
+    SBD_CUDA(cudaMemcpyAsync(S, c->io_b, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int sbdgpu_sigma_device(sbdgpu_ctx* c, const double* dC, double* dS, int precision) {
+  return guarded(c, [&] {
+    if (!dC || !dS) throw Error{SBDGPU_ERR_ARG, "null vector"};
+    check_precision(precision);
+    sigma_ref_convention(c, dC, dS);
+  });
+}
+
+int sbdgpu_last_sigma_ms(sbdgpu_ctx* c, float* ms3) {
+  return guarded(c, [&] {
+    for (int k = 0; k < 3; k++) ms3[k] = c->last_ms[k];
+  });
+}
+
+int sbdgpu_davidson(sbdgpu_ctx* c, const sbdgpu_opts* o, double* Wh, double* energy, double* trace_e,
+                    double* trace_tol, int max_trace, int* n_steps) {
+  return guarded(c, [&] {
+    if (!o || !Wh) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    check_precision(o->precision);
+    int nb = o->max_nb;
+    if (nb < 1 || nb > 32) throw Error{SBDGPU_ERR_ARG, "max_nb must be in [1, 32]"};
+    size_t n = c->N;
+    cudaStream_t st = c->stream;
+    sbdgpu::build_tables(c);
+    sbdgpu::compute_hii(c);
+    sbdgpu::ensure_scratch(c);
+    std::vector<double*> C(nb, nullptr), HC(nb, nullptr);
+    double *W = nullptr, *R = nullptr;
+    struct Free {
+      std::vector<double*>* a;
+      std::vector<double*>* b;
+      double** w;
+      double** r;
+      ~Free() {
+        for (auto p : *a) cudaFree(p);
+        for (auto p : *b) cudaFree(p);
+        cudaFree(*w);
+        cudaFree(*r);
+      }
+    } guard{&C, &HC, &W, &R};
+    for (int k = 0; k < nb; k++) {
+      C[k] = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+      HC[k] = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+    }
+    W = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+    R = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+    SBD_CUDA(cudaMemcpyAsync(W, Wh, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    sbdgpu::apply_phase(c, W);
+    const double eps_reg = 1.0e-12;
+    std::vector<double> H(nb * nb, 0.0), U(nb * nb, 0.0), E(nb, 0.0);
+    std::vector<double> step_times;
+    auto t_start = std::chrono::steady_clock::now();
+    int steps = 0;
+    bool cont = true;
+    for (int it = 0; it < o->max_it && cont; it++) {
+      SBD_CUDA(cudaMemcpyAsync(C[0], W, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+      for (int ib = 0; ib < nb; ib++) {
+        auto t0 = std::chrono::steady_clock::now();
+        sbdgpu::sigma_fp64(c, C[ib], HC[ib]);
+        for (int jb = 0; jb <= ib; jb++) {
+          H[jb + nb * ib] = sbdgpu::dot(c, C[jb], HC[ib], n);
+          H[ib + nb * jb] = H[jb + nb * ib];
+        }
+        for (int jb = 0; jb <= ib; jb++)
+          for (int kb = 0; kb <= ib; kb++) U[jb + nb * kb] = H[jb + nb * kb];
+        sbdgpu::jacobi_eig(ib + 1, U.data(), nb, E.data());
+        sbdgpu::ritz_update(C.data(), HC.data(), U.data(), ib + 1, E[0], W, R, n, st);
+        double nw = std::sqrt(sbdgpu::dot(c, W, W, n));
+        sbdgpu::scale(W, 1.0 / nw, n, st);
+        double tol = std::sqrt(sbdgpu::dot(c, R, R, n));
+        sbdgpu::scale(R, 1.0 / tol, n, st);
+        if (trace_e && steps < max_trace) trace_e[steps] = E[0];
+        if (trace_tol && steps < max_trace) trace_tol[steps] = tol;
+        steps++;
+        if (o->verbose) {
+          // the reference's log line, chemistry/tpb/davidson.h:837-842
+          std::cout << " Davidson iteration " << it << "." << ib << " (tol=" << tol << "):";
+          for (int p = 0; p < std::min(ib + 1, 4); p++) std::cout << " " << E[p];
+          std::cout << std::endl;
+        }
+        if (tol < o->eps) {
+          cont = false;
+          break;
+        }
+        if (ib < nb - 1) {
+          sbdgpu::precondition(R, c->hii, E[0], eps_reg, C[ib + 1], n, st);
+          for (int kb = 0; kb < ib + 1; kb++) {
+            double olap = sbdgpu::dot(c, C[kb], C[ib + 1], n);
+            sbdgpu::axpy(C[ib + 1], C[kb], -olap, n, st);
+          }
+          double nc = std::sqrt(sbdgpu::dot(c, C[ib + 1], C[ib + 1], n));
+          sbdgpu::scale(C[ib + 1], 1.0 / nc, n, st);
+        }
+        SBD_CUDA(cudaStreamSynchronize(st));
+        auto t1 = std::chrono::steady_clock::now();
+        step_times.push_back(std::chrono::duration<double>(t1 - t0).count());
+        double avg = 0.0;
+        for (double x : step_times) avg += x;
+        avg /= step_times.size();
+        double elapsed = std::chrono::duration<double>(t1 - t_start).count();
+        if (elapsed + avg > o->max_time) {  // davidson.h:880-902
+          cont = false;
+          break;
+        }
+      }
+    }
+    // E = <W|HW>, chemistry/tpb/sbdiag.h:239-262
+    sbdgpu::sigma_fp64(c, W, R);
+    double e = sbdgpu::dot(c, W, R, n);
+    sbdgpu::apply_phase(c, W);
+    SBD_CUDA(cudaMemcpyAsync(Wh, W, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    SBD_CUDA(cudaStreamSynchronize(st));
+    if (energy) *energy = e;
+    if (n_steps) *n_steps = steps;
+  });
+}
+
+int sbdgpu_rdm(sbdgpu_ctx* c, const double* Wh, double* one, double* two) {
+  return guarded(c, [&] {
+    if (!Wh || !one || !two) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    sbdgpu::build_tables(c);
+    ensure_io(c);
+    SBD_CUDA(cudaMemcpyAsync(c->io_a, Wh, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    sbdgpu::rdm(c, c->io_a, one, two);
+  });
+}
+
+int sbdgpu_occupation(sbdgpu_ctx* c, const double* Wh, double* dens) {
+  return guarded(c, [&] {
+    if (!Wh || !dens) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    ensure_io(c);
+    SBD_CUDA(cudaMemcpyAsync(c->io_a, Wh, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    sbdgpu::occupation(c, c->io_a, dens);
+  });
+}
+
+int sbdgpu_alpha_weights(sbdgpu_ctx* c, const double* Wh, double* D) {
+  return guarded(c, [&] {
+    if (!Wh || !D) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    ensure_io(c);
+    SBD_CUDA(cudaMemcpyAsync(c->io_a, Wh, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    sbdgpu::alpha_weights(c, c->io_a, c->io_b);
+    SBD_CUDA(cudaMemcpyAsync(D, c->io_b, sizeof(double) * c->na, cudaMemcpyDeviceToHost, c->stream));
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+const char* sbdgpu_last_error(sbdgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void sbdgpu_destroy(sbdgpu_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  sbdgpu::free_tables(c->tab[0]);
+  sbdgpu::free_tables(c->tab[1]);
+  cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);
+  cudaFree(c->hii); cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);
+  for (int k = 0; k < 4; k++)
+    if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,132 @@
+// Internal declarations of the sm_100a tensor-product-basis Davidson path.
+//
+// Data layout in HBM (one context, one device):
+//   strings        uint64 per string, orbital i at bit i, in the caller's order
+//   vectors        FP64 row-major [na][nb], alpha-string-major sign convention
+//                  (the interleaved reference convention differs by the diagonal
+//                  +-1 phase phi(a,b) = (-1)^#{(p in a, r in b): r < p}, applied
+//                  only at the C ABI)
+//   V              (pq|rs) folded over p<->q and r<->s: Vf[pair(p,q)*P + pair(r,s)],
+//                  P = L(L+1)/2, pair(p,q) = max(max+1)/2 + min
+//   tables         per spin, CSR by bra string: singles (ket, packed p/q/pair/sign,
+//                  FP64 string-only matrix element) and doubles (ket, FP64 element);
+//                  plus a sliced-ELL copy of the singles (32 bras per slice, column
+//                  major) for the alpha-beta kernel
+//   J tables       JX[pair(p,q)][i] = sum_{r in string i} (pq|rr): the Coulomb
+//                  coupling of a same-spin single to the other spin's occupation
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sbdgpu.h"
+
+namespace sbdgpu {
+
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define SBD_CUDA(x)                                                                              \
+  do {                                                                                           \
+    cudaError_t e_ = (x);                                                                        \
+    if (e_ != cudaSuccess)                                                                       \
+      throw ::sbdgpu::Error{SBDGPU_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_) +   \
+                                                 " (" + __FILE__ + ":" + std::to_string(__LINE__) + ")"}; \
+  } while (0)
+
+constexpr uint32_t kSellInvalid = 0xFFFFFFFFu;
+constexpr int kSlice = 32;
+
+struct SpinTables {
+  size_t n = 0;
+  int64_t* s_off = nullptr;   // [n+1]
+  int64_t* d_off = nullptr;   // [n+1]
+  int32_t* s_idx = nullptr;   // ket
+  uint32_t* s_info = nullptr; // p | q<<6 | pair<<12 | neg<<31  (p created in bra, q annihilated)
+  double* s_val = nullptr;    // sign * (h_pq + sum_{j in ket} ((pq|jj) - (pj|jq)))
+  int32_t* d_idx = nullptr;
+  double* d_val = nullptr;    // sign * ((p1q1|p2q2) - (p1q2|p2q1))
+  uint64_t ns = 0, nd = 0;
+  int max_s = 0;
+  // sliced ELL of the singles, keyed by bra: ket | pair<<16 | neg<<31
+  size_t nslice = 0;
+  int64_t* sell_off = nullptr;  // [nslice+1]
+  int32_t* sell_w = nullptr;    // [nslice]
+  uint32_t* sell = nullptr;
+  std::vector<int64_t> h_s_off, h_d_off;  // host copies of the offsets
+};
+
+struct Buffers {
+  double* v = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace sbdgpu
+
+struct sbdgpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int L = 0;
+  int P = 0;
+  size_t na = 0, nb = 0, N = 0;
+  double ecore = 0.0;
+  std::vector<uint64_t> h_astr, h_bstr;
+  std::vector<double> h_h1, h_vf;  // host copies
+  uint64_t* astr = nullptr;
+  uint64_t* bstr = nullptr;
+  double* h1 = nullptr;  // [L*L]
+  double* vf = nullptr;  // [P*P]
+  double* ja = nullptr;  // [P][na]
+  double* jb = nullptr;  // [P][nb]
+  double* hii = nullptr; // [N]
+  sbdgpu::SpinTables tab[2];
+  bool tables_ready = false;
+  bool hii_ready = false;
+  // scratch vectors (FP64, N each), allocated on first use
+  double* io_a = nullptr;  // user I/O staging
+  double* io_b = nullptr;
+  double* ct = nullptr;    // transposed C   [nb][na]
+  double* st = nullptr;    // transposed sigma part [nb][na]
+  double* red = nullptr;   // reduction scratch
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float last_ms[3] = {0, 0, 0};
+  std::string err;
+};
+
+namespace sbdgpu {
+
+// tables.cu
+void build_tables(sbdgpu_ctx* c);
+void free_tables(SpinTables& t);
+
+// misc.cu
+void build_j_tables(sbdgpu_ctx* c);
+void compute_hii(sbdgpu_ctx* c);
+void apply_phase(sbdgpu_ctx* c, double* v);
+void transpose(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s);
+void transpose_add(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s);
+double dot(sbdgpu_ctx* c, const double* x, const double* y, size_t n);
+void scale(double* x, double a, size_t n, cudaStream_t s);
+void axpy(double* y, const double* x, double a, size_t n, cudaStream_t s);
+void ritz_update(double* const* C, double* const* HC, const double* U, int nk, double e0, double* W,
+                 double* R, size_t n, cudaStream_t s);
+void precondition(const double* R, const double* hii, double e0, double eps_reg, double* out, size_t n,
+                  cudaStream_t s);
+void rdm(sbdgpu_ctx* c, const double* dW, double* one, double* two);
+void occupation(sbdgpu_ctx* c, const double* dW, double* dens);
+void alpha_weights(sbdgpu_ctx* c, const double* dW, double* D);
+
+// sigma.cu
+void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);
+
+// api.cu
+void ensure_scratch(sbdgpu_ctx* c);
+void ensure_io(sbdgpu_ctx* c);
+void jacobi_eig(int n, double* A, int lda, double* w);
+void* dev_alloc(size_t bytes);
+
+}  // namespace sbdgpu

@@ -1,0 +1,541 @@
+// Diagonal, sign phase, transposes, Davidson vector kernels, occupations and
+// RDMs.  All HBM-bound; the vector kernels are grid-stride loops sized to the
+// 148 SMs.
+#include <cmath>
+#include <cstring>
+
+#include "internal.cuh"
+
+namespace sbdgpu {
+
+namespace {
+
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ int pair_index(int p, int q) {
+  int a = p > q ? p : q, b = p > q ? q : p;
+  return a * (a + 1) / 2 + b;
+}
+
+__global__ void jtable_kernel(const uint64_t* __restrict__ s, int n, const double* __restrict__ vf, int P,
+                              double* __restrict__ J) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int pq = blockIdx.y;
+  if (i >= n) return;
+  uint64_t occ = s[i];
+  double acc = 0.0;
+  while (occ) {
+    int r = __ffsll((long long)occ) - 1;
+    occ &= occ - 1;
+    acc += vf[(size_t)pq * P + pair_index(r, r)];
+  }
+  J[(size_t)pq * n + i] = acc;
+}
+
+// One-spin part of ZeroExcite (chemistry/basic/determinants.h:374-398).
+__global__ void spin_energy_kernel(const uint64_t* __restrict__ s, int n, int L, const double* __restrict__ h1,
+                                   const double* __restrict__ vf, int P, double* __restrict__ E) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t occ = s[i];
+  double e = 0.0;
+  for (uint64_t o1 = occ; o1; o1 &= o1 - 1) {
+    int p = __ffsll((long long)o1) - 1;
+    e += h1[p * L + p];
+    for (uint64_t o2 = o1 & (o1 - 1); o2; o2 &= o2 - 1) {
+      int q = __ffsll((long long)o2) - 1;
+      e += vf[(size_t)pair_index(p, p) * P + pair_index(q, q)] - vf[(size_t)pair_index(p, q) * P + pair_index(p, q)];
+    }
+  }
+  E[i] = e;
+}
+
+// H_ii = E_core + E_alpha(ia) + E_beta(ib) + sum_{p in a, r in b} (pp|rr)
+__global__ void hii_kernel(const uint64_t* __restrict__ astr, size_t na, size_t nb, const double* __restrict__ Ea,
+                           const double* __restrict__ Eb, const double* __restrict__ jb, int P, double ecore,
+                           double* __restrict__ hii) {
+  size_t ia = blockIdx.x;
+  size_t ib = (size_t)blockIdx.y * blockDim.x + threadIdx.x;
+  if (ib >= nb) return;
+  uint64_t occ = astr[ia];
+  double cross = 0.0;
+  while (occ) {
+    int p = __ffsll((long long)occ) - 1;
+    occ &= occ - 1;
+    cross += jb[(size_t)pair_index(p, p) * nb + ib];
+  }
+  hii[ia * nb + ib] = ecore + Ea[ia] + Eb[ib] + cross;
+}
+
+__global__ void phase_kernel(const uint64_t* __restrict__ astr, const uint64_t* __restrict__ bstr, size_t nb,
+                             double* __restrict__ v) {
+  size_t ia = blockIdx.x;
+  size_t ib = (size_t)blockIdx.y * blockDim.x + threadIdx.x;
+  if (ib >= nb) return;
+  uint64_t a = astr[ia], b = bstr[ib];
+  int cnt = 0;
+  while (a) {
+    int p = __ffsll((long long)a) - 1;
+    a &= a - 1;
+    cnt += __popcll(b & ((1ull << p) - 1ull));
+  }
+  if (cnt & 1) v[ia * nb + ib] = -v[ia * nb + ib];
+}
+
+template <bool kAdd>
+__global__ void transpose_kernel(const double* __restrict__ in, double* __restrict__ out, size_t rows,
+                                 size_t cols) {
+  __shared__ double tile[32][33];
+  size_t c0 = (size_t)blockIdx.x * 32, r0 = (size_t)blockIdx.y * 32;
+  int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  for (int k = ty; k < 32; k += 8) {
+    size_t r = r0 + k, c = c0 + tx;
+    if (r < rows && c < cols) tile[k][tx] = in[r * cols + c];
+  }
+  __syncthreads();
+  for (int k = ty; k < 32; k += 8) {
+    size_t c = c0 + k, r = r0 + tx;  // out[c][r]
+    if (r < rows && c < cols) {
+      if (kAdd)
+        out[c * rows + r] += tile[tx][k];
+      else
+        out[c * rows + r] = tile[tx][k];
+    }
+  }
+}
+
+__global__ void dot_partial(const double* __restrict__ x, const double* __restrict__ y, size_t n,
+                            double* __restrict__ part) {
+  __shared__ double sh[kRedThreads / 32];
+  double acc = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    acc += x[i] * y[i];
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kRedThreads / 32; w++) s += sh[w];
+    part[blockIdx.x] = s;
+  }
+}
+
+__global__ void dot_final(const double* __restrict__ part, int np, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += part[i];
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); w++) s += sh[w];
+    *out = s;
+  }
+}
+
+__global__ void scale_kernel(double* x, double a, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+
+__global__ void axpy_kernel(double* y, const double* x, double a, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] += x[i] * a;
+}
+
+struct PtrPack {
+  const double* p[32];
+  double u[32];
+};
+
+// W = sum_k U_k C_k ; R = E0*W - sum_k U_k HC_k  (davidson.h:772-797)
+__global__ void ritz_kernel(PtrPack c, PtrPack hc, int nk, double e0, double* __restrict__ W,
+                            double* __restrict__ R, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double w = 0.0, r = 0.0;
+    for (int k = 0; k < nk; k++) {
+      w += c.p[k][i] * c.u[k];
+      r -= hc.p[k][i] * c.u[k];
+    }
+    W[i] = w;
+    R[i] = r + e0 * w;
+  }
+}
+
+// C_new = R / (E0 - H_ii), regularised as davidson.h:855-862
+__global__ void precond_kernel(const double* __restrict__ R, const double* __restrict__ hii, double e0,
+                               double eps_reg, double* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double den = e0 - hii[i];
+    out[i] = fabs(den) > eps_reg ? R[i] / den : R[i] / (den - eps_reg);
+  }
+}
+
+// ---------------------------------------------------------------- RDMs
+
+struct Det {
+  uint64_t lo, hi;  // interleaved spin orbitals 0..63 and 64..127
+};
+
+__device__ __forceinline__ uint64_t spread32(uint64_t x) {
+  x &= 0xFFFFFFFFull;
+  x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+  x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+  x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+  x = (x | (x << 2)) & 0x3333333333333333ull;
+  x = (x | (x << 1)) & 0x5555555555555555ull;
+  return x;
+}
+
+// DetFromAlphaBeta, chemistry/basic/determinants.h:98-119
+__device__ __forceinline__ Det interleave(uint64_t a, uint64_t b) {
+  Det d;
+  d.lo = spread32(a) | (spread32(b) << 1);
+  d.hi = spread32(a >> 32) | (spread32(b >> 32) << 1);
+  return d;
+}
+
+__device__ __forceinline__ uint64_t low_mask(int k) {  // bits [0,k) of a 64-bit word, k in [0,64]
+  return k >= 64 ? ~0ull : ((1ull << k) - 1ull);
+}
+
+// occupied spin orbitals strictly between x and y
+__device__ __forceinline__ double parity(const Det& d, int x, int y) {
+  int lo = x < y ? x : y, hi = x < y ? y : x;
+  int cnt = 0;
+  if (hi - lo >= 2) {
+    int a = lo + 1, b = hi;  // [a, b)
+    uint64_t mlo = low_mask(b < 64 ? b : 64) & ~low_mask(a < 64 ? a : 64);
+    uint64_t mhi = low_mask(b > 64 ? b - 64 : 0) & ~low_mask(a > 64 ? a - 64 : 0);
+    cnt = __popcll(d.lo & mlo) + __popcll(d.hi & mhi);
+  }
+  return (cnt & 1) ? -1.0 : 1.0;
+}
+
+// OneDiffCorrelation, chemistry/tpb/correlation.h:49-86 (det = bra, i created, a annihilated)
+__device__ void one_diff(const Det& det, double v0, int i, int a, int L, double* one, double* two) {
+  size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
+  double v = v0 * parity(det, i, a);
+  int oi = i / 2, si = i % 2, oa = a / 2;
+  atomicAdd(&one[si * L2 + oi + (size_t)L * oa], v);
+  for (int w = 0; w < 2; w++) {
+    uint64_t bits = w ? det.hi : det.lo;
+    while (bits) {
+      int soj = (__ffsll((long long)bits) - 1) + 64 * w;
+      bits &= bits - 1;
+      int oj = soj / 2, sj = soj % 2;
+      atomicAdd(&two[(si + 2 * sj) * L4 + oa + oj * L + oi * L2 + oj * L3], v);
+      atomicAdd(&two[(sj + 2 * si) * L4 + oj + oa * L + oj * L2 + oi * L3], v);
+      if (si == sj) {
+        atomicAdd(&two[(si + 2 * sj) * L4 + oa + oj * L + oj * L2 + oi * L3], -v);
+        atomicAdd(&two[(sj + 2 * si) * L4 + oj + oa * L + oi * L2 + oj * L3], -v);
+      }
+    }
+  }
+}
+
+// TwoDiffCorrelation, chemistry/tpb/correlation.h:91-130
+__device__ void two_diff(const Det& det, double v0, int i, int j, int a, int b, int L, double* two) {
+  size_t L2 = (size_t)L * L, L4 = L2 * L2;
+  int I = i < j ? i : j, J = i < j ? j : i, A = a < b ? a : b, B = a < b ? b : a;
+  double sgn = parity(det, I, A) * parity(det, J, B);
+  if (A > J || B < I) sgn = -sgn;
+  int oi = I / 2, si = I % 2, oa = A / 2, sa = A % 2, oj = J / 2, sj = J % 2, ob = B / 2, sb = B % 2;
+  double v = sgn * v0;
+  if (si == sa) {
+    atomicAdd(&two[(si + 2 * sj) * L4 + oa + L * ob + L2 * (oi + (size_t)L * oj)], v);
+    atomicAdd(&two[(sj + 2 * si) * L4 + ob + L * oa + L2 * (oj + (size_t)L * oi)], v);
+  }
+  if (si == sb) {
+    atomicAdd(&two[(si + 2 * sj) * L4 + oa + L * ob + L2 * (oj + (size_t)L * oi)], -v);
+    atomicAdd(&two[(sj + 2 * si) * L4 + ob + L * oa + L2 * (oi + (size_t)L * oj)], -v);
+  }
+}
+
+__device__ __forceinline__ int take_bits(const Det& m, int* out) {
+  int n = 0;
+  uint64_t x = m.lo;
+  while (x && n < 3) {
+    out[n++] = __ffsll((long long)x) - 1;
+    x &= x - 1;
+  }
+  x = m.hi;
+  while (x && n < 3) {
+    out[n++] = 64 + __ffsll((long long)x) - 1;
+    x &= x - 1;
+  }
+  return n;
+}
+
+// CorrelationTermAddition, chemistry/tpb/correlation.h:135-189 (off-diagonal kinds)
+__device__ void term(const Det& bra, const Det& ket, double v0, int L, double* one, double* two) {
+  Det cm{bra.lo & ~ket.lo, bra.hi & ~ket.hi}, dm{ket.lo & ~bra.lo, ket.hi & ~bra.hi};
+  int c[3], d[3];
+  int nc = take_bits(cm, c);
+  take_bits(dm, d);
+  if (nc == 1)
+    one_diff(bra, v0, c[0], d[0], L, one, two);
+  else if (nc == 2)
+    two_diff(bra, v0, c[0], c[1], d[0], d[1], L, two);
+}
+
+__global__ void rdm_kernel(const uint64_t* __restrict__ astr, const uint64_t* __restrict__ bstr, size_t na,
+                           size_t nb, int L, const double* __restrict__ W, SpinTables ta, SpinTables tb,
+                           double* one, double* two) {
+  size_t ia = blockIdx.x;
+  size_t ib = (size_t)blockIdx.y * blockDim.x + threadIdx.x;
+  if (ib >= nb) return;
+  double wi = W[ia * nb + ib];
+  if (wi == 0.0) return;
+  Det bra = interleave(astr[ia], bstr[ib]);
+  for (int kind = 0; kind < 2; kind++) {
+    const int64_t* off = kind ? ta.d_off : ta.s_off;
+    const int32_t* idx = kind ? ta.d_idx : ta.s_idx;
+    for (int64_t k = off[ia]; k < off[ia + 1]; k++) {
+      size_t ja = idx[k];
+      term(bra, interleave(astr[ja], bstr[ib]), wi * W[ja * nb + ib], L, one, two);
+    }
+  }
+  for (int kind = 0; kind < 2; kind++) {
+    const int64_t* off = kind ? tb.d_off : tb.s_off;
+    const int32_t* idx = kind ? tb.d_idx : tb.s_idx;
+    for (int64_t k = off[ib]; k < off[ib + 1]; k++) {
+      size_t jb = idx[k];
+      term(bra, interleave(astr[ia], bstr[jb]), wi * W[ia * nb + jb], L, one, two);
+    }
+  }
+  for (int64_t k = ta.s_off[ia]; k < ta.s_off[ia + 1]; k++) {
+    size_t ja = ta.s_idx[k];
+    for (int64_t m = tb.s_off[ib]; m < tb.s_off[ib + 1]; m++) {
+      size_t jb = tb.s_idx[m];
+      term(bra, interleave(astr[ja], bstr[jb]), wi * W[ja * nb + jb], L, one, two);
+    }
+  }
+}
+
+// Per alpha row: D[ia] = sum_ib W^2 and X[ia][r] = sum_ib W^2 n_r(beta string ib)
+__global__ void row_weights_kernel(const double* __restrict__ W, const uint64_t* __restrict__ bstr, size_t nb,
+                                   int L, double* __restrict__ D, double* __restrict__ X) {
+  __shared__ double acc[65];
+  size_t ia = blockIdx.x;
+  for (int r = threadIdx.x; r < 65; r += blockDim.x) acc[r] = 0.0;
+  __syncthreads();
+  double tot = 0.0;
+  for (size_t ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+    double w = W[ia * nb + ib];
+    double w2 = w * w;
+    if (w2 == 0.0) continue;
+    tot += w2;
+    if (X) {
+      uint64_t occ = bstr[ib];
+      while (occ) {
+        int r = __ffsll((long long)occ) - 1;
+        occ &= occ - 1;
+        atomicAdd(&acc[r], w2);
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&acc[64], tot);
+  __syncthreads();
+  if (threadIdx.x == 0) D[ia] = acc[64];
+  if (X)
+    for (int r = threadIdx.x; r < L; r += blockDim.x) X[ia * L + r] = acc[r];
+}
+
+__global__ void col_weights_kernel(const double* __restrict__ W, size_t na, size_t nb, double* __restrict__ D) {
+  size_t ib = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ib >= nb) return;
+  double acc = 0.0;
+  for (size_t ia = 0; ia < na; ia++) {
+    double w = W[ia * nb + ib];
+    acc += w * w;
+  }
+  D[ib] = acc;
+}
+
+inline int grid_for(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)(b < 148 * 8 ? (b ? b : 1) : 148 * 8);
+}
+
+}  // namespace
+
+void build_j_tables(sbdgpu_ctx* c) {
+  if (c->ja) return;
+  c->ja = (double*)dev_alloc(sizeof(double) * c->P * c->na);
+  c->jb = (double*)dev_alloc(sizeof(double) * c->P * c->nb);
+  dim3 ga((unsigned)((c->na + 255) / 256), (unsigned)c->P);
+  jtable_kernel<<<ga, 256, 0, c->stream>>>(c->astr, (int)c->na, c->vf, c->P, c->ja);
+  dim3 gb((unsigned)((c->nb + 255) / 256), (unsigned)c->P);
+  jtable_kernel<<<gb, 256, 0, c->stream>>>(c->bstr, (int)c->nb, c->vf, c->P, c->jb);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void compute_hii(sbdgpu_ctx* c) {
+  if (c->hii_ready) return;
+  build_j_tables(c);
+  double* Ea = (double*)dev_alloc(sizeof(double) * (c->na + c->nb));
+  double* Eb = Ea + c->na;
+  spin_energy_kernel<<<(unsigned)((c->na + 255) / 256), 256, 0, c->stream>>>(c->astr, (int)c->na, c->L, c->h1,
+                                                                             c->vf, c->P, Ea);
+  spin_energy_kernel<<<(unsigned)((c->nb + 255) / 256), 256, 0, c->stream>>>(c->bstr, (int)c->nb, c->L, c->h1,
+                                                                             c->vf, c->P, Eb);
+  if (!c->hii) c->hii = (double*)dev_alloc(sizeof(double) * c->N);
+  dim3 g((unsigned)c->na, (unsigned)((c->nb + 255) / 256));
+  hii_kernel<<<g, 256, 0, c->stream>>>(c->astr, c->na, c->nb, Ea, Eb, c->jb, c->P, c->ecore, c->hii);
+  SBD_CUDA(cudaGetLastError());
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(Ea);
+  c->hii_ready = true;
+}
+
+void apply_phase(sbdgpu_ctx* c, double* v) {
+  dim3 g((unsigned)c->na, (unsigned)((c->nb + 255) / 256));
+  phase_kernel<<<g, 256, 0, c->stream>>>(c->astr, c->bstr, c->nb, v);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void transpose(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s) {
+  dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+  transpose_kernel<false><<<g, dim3(32, 8), 0, s>>>(in, out, rows, cols);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void transpose_add(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s) {
+  dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+  transpose_kernel<true><<<g, dim3(32, 8), 0, s>>>(in, out, rows, cols);
+  SBD_CUDA(cudaGetLastError());
+}
+
+double dot(sbdgpu_ctx* c, const double* x, const double* y, size_t n) {
+  ensure_scratch(c);
+  dot_partial<<<kRedBlocks, kRedThreads, 0, c->stream>>>(x, y, n, c->red);
+  dot_final<<<1, 1024, 0, c->stream>>>(c->red, kRedBlocks, c->red + kRedBlocks);
+  SBD_CUDA(cudaGetLastError());
+  double r = 0.0;
+  SBD_CUDA(cudaMemcpyAsync(&r, c->red + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+  return r;
+}
+
+void scale(double* x, double a, size_t n, cudaStream_t s) {
+  scale_kernel<<<grid_for(n), 256, 0, s>>>(x, a, n);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void axpy(double* y, const double* x, double a, size_t n, cudaStream_t s) {
+  axpy_kernel<<<grid_for(n), 256, 0, s>>>(y, x, a, n);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void ritz_update(double* const* C, double* const* HC, const double* U, int nk, double e0, double* W, double* R,
+                 size_t n, cudaStream_t s) {
+  PtrPack pc{}, ph{};
+  for (int k = 0; k < nk; k++) {
+    pc.p[k] = C[k];
+    ph.p[k] = HC[k];
+    pc.u[k] = U[k];
+  }
+  ritz_kernel<<<grid_for(n), 256, 0, s>>>(pc, ph, nk, e0, W, R, n);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void precondition(const double* R, const double* hii, double e0, double eps_reg, double* out, size_t n,
+                  cudaStream_t s) {
+  precond_kernel<<<grid_for(n), 256, 0, s>>>(R, hii, e0, eps_reg, out, n);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void alpha_weights(sbdgpu_ctx* c, const double* dW, double* D) {
+  row_weights_kernel<<<(unsigned)c->na, 256, 0, c->stream>>>(dW, c->bstr, c->nb, c->L, D, nullptr);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void occupation(sbdgpu_ctx* c, const double* dW, double* dens) {
+  double* Da = (double*)dev_alloc(sizeof(double) * (c->na + c->nb));
+  double* Db = Da + c->na;
+  alpha_weights(c, dW, Da);
+  col_weights_kernel<<<(unsigned)((c->nb + 255) / 256), 256, 0, c->stream>>>(dW, c->na, c->nb, Db);
+  SBD_CUDA(cudaGetLastError());
+  std::vector<double> hd(c->na + c->nb);
+  SBD_CUDA(cudaMemcpyAsync(hd.data(), Da, sizeof(double) * hd.size(), cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(Da);
+  int L = c->L;
+  for (int i = 0; i < 2 * L; i++) dens[i] = 0.0;
+  for (size_t ia = 0; ia < c->na; ia++)
+    for (int p = 0; p < L; p++)
+      if ((c->h_astr[ia] >> p) & 1) dens[2 * p] += hd[ia];
+  for (size_t ib = 0; ib < c->nb; ib++)
+    for (int p = 0; p < L; p++)
+      if ((c->h_bstr[ib] >> p) & 1) dens[2 * p + 1] += hd[c->na + ib];
+}
+
+void rdm(sbdgpu_ctx* c, const double* dW, double* one, double* two) {
+  int L = c->L;
+  size_t L2 = (size_t)L * L, L4 = L2 * L2;
+  double* d_one = (double*)dev_alloc(sizeof(double) * (2 * L2 + 4 * L4));
+  double* d_two = d_one + 2 * L2;
+  SBD_CUDA(cudaMemsetAsync(d_one, 0, sizeof(double) * (2 * L2 + 4 * L4), c->stream));
+  dim3 g((unsigned)c->na, (unsigned)((c->nb + 127) / 128));
+  rdm_kernel<<<g, 128, 0, c->stream>>>(c->astr, c->bstr, c->na, c->nb, L, dW, c->tab[0], c->tab[1], d_one, d_two);
+  SBD_CUDA(cudaGetLastError());
+  // diagonal contributions (ZeroDiffCorrelation, correlation.h:15-44) from the
+  // alpha-row weights, beta-column weights and the alpha x beta occupation moment
+  double* Da = (double*)dev_alloc(sizeof(double) * (c->na + c->nb + c->na * L));
+  double* Db = Da + c->na;
+  double* X = Db + c->nb;
+  row_weights_kernel<<<(unsigned)c->na, 256, 0, c->stream>>>(dW, c->bstr, c->nb, L, Da, X);
+  col_weights_kernel<<<(unsigned)((c->nb + 255) / 256), 256, 0, c->stream>>>(dW, c->na, c->nb, Db);
+  SBD_CUDA(cudaGetLastError());
+  std::vector<double> h(c->na + c->nb + c->na * L);
+  SBD_CUDA(cudaMemcpyAsync(h.data(), Da, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaMemcpyAsync(one, d_one, sizeof(double) * 2 * L2, cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaMemcpyAsync(two, d_two, sizeof(double) * 4 * L4, cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+  cudaFree(d_one);
+  cudaFree(Da);
+  const double* hDa = h.data();
+  const double* hDb = hDa + c->na;
+  const double* hX = hDb + c->nb;
+  std::vector<double> Aaa(L2, 0.0), Abb(L2, 0.0), M(L2, 0.0), na1(L, 0.0), nb1(L, 0.0);
+  for (size_t ia = 0; ia < c->na; ia++) {
+    uint64_t a = c->h_astr[ia];
+    for (int p = 0; p < L; p++) {
+      if (!((a >> p) & 1)) continue;
+      na1[p] += hDa[ia];
+      for (int r = 0; r < L; r++) M[p * L + r] += hX[ia * L + r];
+      for (int q = 0; q < L; q++)
+        if (q != p && ((a >> q) & 1)) Aaa[p * L + q] += hDa[ia];
+    }
+  }
+  for (size_t ib = 0; ib < c->nb; ib++) {
+    uint64_t b = c->h_bstr[ib];
+    for (int p = 0; p < L; p++) {
+      if (!((b >> p) & 1)) continue;
+      nb1[p] += hDb[ib];
+      for (int q = 0; q < L; q++)
+        if (q != p && ((b >> q) & 1)) Abb[p * L + q] += hDb[ib];
+    }
+  }
+  size_t L3 = L2 * L;
+  for (int p = 0; p < L; p++) {
+    one[0 * L2 + p + (size_t)L * p] += na1[p];
+    one[1 * L2 + p + (size_t)L * p] += nb1[p];
+    for (int q = 0; q < L; q++) {
+      // same-spin pairs (each unordered pair contributes both orders)
+      two[0 * L4 + p + L * q + L2 * p + L3 * q] += Aaa[p * L + q];
+      two[0 * L4 + p + L * q + L2 * q + L3 * p] -= Aaa[p * L + q];
+      two[3 * L4 + p + L * q + L2 * p + L3 * q] += Abb[p * L + q];
+      two[3 * L4 + p + L * q + L2 * q + L3 * p] -= Abb[p * L + q];
+      // opposite-spin pairs (alpha p, beta q)
+      two[2 * L4 + p + L * q + L2 * p + L3 * q] += M[p * L + q];
+      two[1 * L4 + q + L * p + L2 * q + L3 * p] += M[p * L + q];
+    }
+  }
+}
+
+}  // namespace sbdgpu

@@ -1,0 +1,146 @@
+"""CUDA path against the reference: golden fixtures made by the reference
+itself, and the C restatement (oracle) on seeded cases.
+
+Bars: excitation tables bit-exact; H_ii and sigma element-wise within
+1e-12 * max|ref|; Davidson energy within 1e-10 Eh; RDMs and occupations within
+1e-10."""
+import numpy as np
+import pytest
+
+import oracle
+import sbd_b200
+from sbd_b200 import synth
+from conftest import golden_integrals, seeded_vector
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_ctx(g):
+    fd = golden_integrals(g)
+    ints = synth.Integrals(int(g["norb"]), fd.ecore, fd.h, fd.eri)
+    return sbd_b200.context_from_integrals(ints, g["astr"], g["bstr"])
+
+
+def test_tables(golden):
+    ctx = gpu_ctx(golden)
+    for spin, s in ((0, "a"), (1, "b")):
+        so, si, do, di = ctx.tables(spin)
+        assert np.array_equal(so, golden[f"t_{s}s_off"])
+        assert np.array_equal(si, golden[f"t_{s}s_idx"].astype(np.uint64))
+        assert np.array_equal(do, golden[f"t_{s}d_off"])
+        assert np.array_equal(di, golden[f"t_{s}d_idx"].astype(np.uint64))
+
+
+def test_hii(golden):
+    ctx = gpu_ctx(golden)
+    ref = golden["hii"]
+    assert np.abs(ctx.hii() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_sigma(golden):
+    ctx = gpu_ctx(golden)
+    n = ctx.n
+    C = seeded_vector(n, int(golden["C_seed"]))
+    r0, r1 = (int(x) for x in golden["sigma_rows"])
+    s = ctx.sigma(C)[r0 * ctx.nb:r1 * ctx.nb]
+    ref = golden["sigma"]
+    assert np.abs(s - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_davidson(golden):
+    if "energy" not in golden:
+        pytest.skip("fixture has no Davidson result")
+    ctx = gpu_ctx(golden)
+    W0 = np.zeros(ctx.n)
+    W0[0] = 1.0
+    e, W, te, tt = ctx.davidson(W0, 1000, 10, 1e-8)
+    assert abs(e - float(golden["energy"])) < 1e-10
+    tr = golden["trace"]
+    assert len(te) == len(tr)
+    np.testing.assert_allclose(tt, tr[:, 2], rtol=2e-5)
+    np.testing.assert_allclose(te, tr[:, 3], rtol=2e-6)
+    assert abs(abs(np.dot(W, golden["W"])) - 1.0) < 1e-10
+    np.testing.assert_allclose(ctx.occupation(W), golden["density"], atol=1e-10)
+
+
+def test_rdm(golden):
+    if "rdm1" not in golden:
+        pytest.skip("fixture has no RDMs")
+    ctx = gpu_ctx(golden)
+    one, two = ctx.rdm(golden["W"])
+    assert np.abs(one - golden["rdm1"]).max() < 1e-10
+    assert np.abs(two - golden["rdm2"]).max() < 1e-10
+
+
+def _seeded_system(norb, ne, count, seed, ragged=False):
+    ints, ne, strs = synth.make_small(norb, ne, count, seed)
+    a = strs
+    b = strs
+    if ragged:
+        b = synth.selected_strings(norb, ne, max(8, len(strs) // 3), np.diag(ints.h), seed + 7) \
+            if count is not None else strs[: max(1, len(strs) // 2)]
+    return ints, np.asarray(a, np.uint64), np.asarray(b, np.uint64)
+
+
+@pytest.mark.parametrize("norb,ne,count,seed,ragged", [
+    (14, 4, 300, 11, False),
+    (16, 5, 400, 12, True),
+    (20, 3, 600, 13, False),
+])
+def test_sigma_vs_oracle_seeded(norb, ne, count, seed, ragged):
+    ints, a, b = _seeded_system(norb, ne, count, seed, ragged)
+    ctx = sbd_b200.context_from_integrals(ints, a, b)
+    orc = oracle.Oracle(norb, a, b, ints.ecore, ints.h, ints.eri)
+    C = seeded_vector(ctx.n, seed)
+    s = ctx.sigma(C)
+    rows = (0, min(len(a), 24))
+    ref = orc.sigma(C, rows)
+    got = s[rows[0] * ctx.nb:rows[1] * ctx.nb]
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    np.testing.assert_allclose(ctx.hii(), orc.hii(), rtol=1e-12, atol=1e-12)
+    for spin in (0, 1):
+        so, si, do, di = ctx.tables(spin)
+        o1, i1 = orc.table(spin, 0)
+        o2, i2 = orc.table(spin, 1)
+        assert np.array_equal(so, o1) and np.array_equal(si, i1)
+        assert np.array_equal(do, o2) and np.array_equal(di, i2)
+
+
+def test_edge_cases():
+    # one alpha string, unrelated beta strings with no in-set excitations
+    ints = synth.make_integrals(10, 5)
+    a = np.array([0b0000000111], np.uint64)
+    b = np.array([0b0000000111, 0b0111000000], np.uint64)  # distance 6: no singles/doubles
+    ctx = sbd_b200.context_from_integrals(ints, a, b)
+    orc = oracle.Oracle(10, a, b, ints.ecore, ints.h, ints.eri)
+    C = np.array([0.6, 0.8])
+    np.testing.assert_allclose(ctx.sigma(C), orc.sigma(C), rtol=1e-12, atol=1e-13)
+    so, si, do, di = ctx.tables(1)
+    assert len(si) == 0 and len(di) == 0
+    # a single determinant: sigma = H_ii * C
+    ctx1 = sbd_b200.context_from_integrals(ints, a, a)
+    np.testing.assert_allclose(ctx1.sigma(np.array([2.0])), 2.0 * orc.hii()[:1], rtol=1e-13)
+
+
+def test_invalid_inputs_rejected():
+    ints = synth.make_integrals(6, 1)
+    with pytest.raises(sbd_b200.SbdGpuError):
+        sbd_b200.context_from_integrals(ints, np.array([1 << 7], np.uint64), np.array([1], np.uint64))
+    ctx = sbd_b200.context_from_integrals(ints, np.array([3, 5], np.uint64), np.array([3, 5], np.uint64))
+    with pytest.raises(sbd_b200.SbdGpuError):
+        ctx.sigma(np.ones(4), precision=99)
+    with pytest.raises(sbd_b200.SbdGpuError):
+        ctx.davidson(np.ones(4), 1, 64, 1e-8)
+
+
+def test_sigma_symmetric_and_linear_at_scale():
+    """Size-independent properties on a 4000 x 4000 selected basis (16M
+    determinants, norb 26, 6 alpha/6 beta): <x|Hy> = <Hx|y> and linearity."""
+    ints, ne, strs = synth.make_workload("c1_L26_6e_4000", seed=0)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs)
+    x = seeded_vector(ctx.n, 1)
+    y = seeded_vector(ctx.n, 2)
+    hx, hy = ctx.sigma(x), ctx.sigma(y)
+    assert abs(np.dot(x, hy) - np.dot(hx, y)) < 1e-10 * abs(np.dot(x, hy)) + 1e-12
+    hxy = ctx.sigma(0.5 * x - 2.0 * y)
+    assert np.abs(hxy - (0.5 * hx - 2.0 * hy)).max() < 1e-11 * np.abs(hxy).max()
