@@ -1,0 +1,338 @@
+"""Benchmark: sigma builds per second on the 144M-determinant workload.
+
+Workload: norb 36, 8 alpha / 8 beta electrons, 12,000 x 12,000 selected
+strings (144,000,000 determinants): every string of excitation rank <= 2 from
+aufbau plus seeded higher-rank strings, seeded synthetic integrals (the
+reference ships no usable input; see sbd_b200/synth.py).  A step is one full
+sigma = H*C build on a normalised N(0,1) vector, in FP64.
+
+  value   sigma/s with C and sigma resident in HBM (CUDA events on the
+          library's stream around each build); the 1.15 GB vectors are far
+          larger than the 126 MB L2, so no flush is needed between steps
+  e2e     sigma/s through the C ABI call a user makes with host buffers
+          (sbdgpu_sigma: pinned host C -> device, build, device -> host sigma)
+
+--impl reference times the reference's own CPU mult (r-ccs-cms/sbd compiled at
+MPI world size 1 into oracle/_ref/libsbdref.so) on a bounded slice of alpha
+rows of the same workload with all host threads, extrapolated to a full build.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = "c2_L36_8e_12000"
+METRIC = "sigma builds/s at 144M determinants"
+UNIT = "sigma/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+LAUNCHES_PER_SIGMA = 7  # phase, rows(alpha), transpose, rows(beta), transpose-add, alpha-beta, phase
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self._proc = None
+            return
+        threading.Thread(target=self._read, daemon=True).start()
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def table_stats(ctx):
+    st = {}
+    for spin in (0, 1):
+        so, si, do, di = ctx.tables(spin)
+        st[spin] = (len(si), len(di))
+    return st
+
+
+def algorithmic(ctx, st):
+    """Per-sigma flops 2*nnz(H) and compulsory bytes (vectors + tables)."""
+    na, nb, n = ctx.na, ctx.nb, ctx.n
+    nsa, nda = st[0]
+    nsb, ndb = st[1]
+    nnz = n + nb * (nsa + nda) + na * (nsb + ndb) + nsa * nsb
+    table_bytes = (nsa + nsb) * (4 + 4 + 8) + (nda + ndb) * (4 + 8)
+    sigma_bytes = 8 * n * 3 + table_bytes  # read C, read H_ii, write sigma
+    # alpha-beta kernel alone: C read once, sigma read-modify-write, beta singles
+    # (sliced ELL, 4 B) and alpha singles (16 B) read once
+    ab_bytes = 8 * n * 3 + nsb * 4 + nsa * 16
+    return {"flops": 2.0 * nnz, "nnz": nnz, "sigma_bytes": sigma_bytes, "ab_bytes": ab_bytes,
+            "ab_flops": 2.0 * nsa * nsb}
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class RefSampler:
+    """The reference's own CPU mult on slices of alpha rows of the workload,
+    extrapolated linearly in rows to a full sigma build (rows are independent;
+    slices at the start, middle and end of the row range)."""
+
+    def __init__(self, ints, ne, strs):
+        import oracle
+        from sbd_b200 import synth
+        self._td = tempfile.TemporaryDirectory()
+        fp, dp = synth.write_workload(self._td.name, ints, ne, strs)
+        t0 = time.perf_counter()
+        self.ref = oracle.Reference(fp, dp)
+        self.t_setup = time.perf_counter() - t0
+        self.na = self.ref.na
+        C = np.random.default_rng(1234).normal(size=self.ref.na * self.ref.nb)
+        self.C = C / np.linalg.norm(C)
+        t = time.perf_counter()
+        self.ref.sigma(self.C, (0, 1))
+        self.per_row = time.perf_counter() - t
+
+    def sample(self, budget_s: float) -> dict:
+        starts = [0, self.na // 2, max(0, self.na - 1)]
+        rows_each = max(1, int(budget_s / max(self.per_row, 1e-3) / len(starts)))
+        total_rows, total_t = 0, 0.0
+        for s in starts:
+            r1 = min(self.na, s + rows_each)
+            t = time.perf_counter()
+            self.ref.sigma(self.C, (s, r1))
+            total_t += time.perf_counter() - t
+            total_rows += r1 - s
+        sec = total_t / total_rows * self.na
+        return {"value": 1.0 / sec, "unit": UNIT, "cores": host_cores(), "kind": "reference",
+                "sample": f"reference mult (r-ccs-cms/sbd, OpenMP, MPI world size 1) on {total_rows} of "
+                          f"{self.na} alpha rows in 3 slices (start/middle/end), {total_t:.1f} s, "
+                          f"extrapolated linearly in rows; reference table build {self.t_setup:.1f} s"}
+
+    def close(self):
+        self.ref.close()
+        self._td.cleanup()
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    from sbd_b200 import synth
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsbdref.so was not built"}))
+        return 0
+    ints, ne, strs = synth.make_workload(args.workload, seed=0)
+    rs = RefSampler(ints, ne, strs)
+    per = max(2.0, args.ref_budget * 6 / (args.warmup + args.steps))
+    vals, base = [], None
+    for i in range(args.warmup + args.steps):
+        r = rs.sample(per)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            base = r
+    rs.close()
+    v = statistics.mean(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded integrals and strings)", "impl": "reference",
+            "config": {"workload": args.workload, "determinants": int(len(strs)) ** 2, "norb": ints.norb,
+                       "electrons": f"{ne}a/{ne}b", "strings_per_spin": int(len(strs)),
+                       "parallelism": f"OpenMP x{host_cores()}, MPI world size 1"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": base["cores"], "kind": "reference",
+                             "sample": base["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_gpu(args):
+    import torch
+    import sbd_b200
+    from sbd_b200 import synth
+
+    rank, world, local = dist_env()
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    ints, ne, strs = synth.make_workload(args.workload, seed=0)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    st = table_stats(ctx)
+    alg = algorithmic(ctx, st)
+    n = ctx.n
+    C = torch.randn(n, dtype=torch.float64, device=f"cuda:{dev}", generator=torch.Generator(device=f"cuda:{dev}").manual_seed(1))
+    C /= torch.linalg.norm(C)
+    S = torch.empty_like(C)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        ctx.sigma_device(C.data_ptr(), S.data_ptr())
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    tot, ab, parts = 0.0, 0.0, [0.0, 0.0, 0.0]
+    for _ in range(args.steps):
+        ctx.sigma_device(C.data_ptr(), S.data_ptr())
+        ms = ctx.last_sigma_ms()
+        tot += ms[3]
+        for k in range(3):
+            parts[k] += ms[k]
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    # end to end: pinned host buffers through the C ABI
+    Ch = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    Ch.copy_(C.cpu())
+    Sh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    e2e_ms = 0.0
+    Cnp = Ch.numpy()
+    Snp = Sh.numpy()
+    import ctypes
+    for _ in range(args.steps):
+        rc = sbd_b200.lib().sbdgpu_sigma(ctx._h, Cnp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                         Snp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0)
+        ctx._check(rc)
+        e2e_ms += ctx.last_sigma_ms()[4]
+    torch.cuda.synchronize()
+    sampler.stop()
+    if pg:
+        pg.barrier()
+    t_step = tot / args.steps
+    t_e2e = e2e_ms / args.steps
+    if pg:
+        tt = torch.tensor([t_step, t_e2e], dtype=torch.float64, device=f"cuda:{dev}")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_step, t_e2e = tt.tolist()
+    if rank != 0:
+        ctx.close()
+        if pg:
+            pg.destroy_process_group()
+        return 0
+    hbm_peak, peak_kind = measured_peaks()
+    ab_ms = parts[2] / args.steps
+    kernel_names = ["rows_kernel<true> (diag + alpha same-spin)", "beta same-spin (transpose, rows_kernel<false>, transpose-add)",
+                    "ab_kernel (alpha-beta)"]
+    dom = int(np.argmax(parts))
+    dom_ms = parts[dom] / args.steps
+    dom_bytes = [8.0 * n * 3 + st[0][0] * 16 + st[0][1] * 12, 8.0 * n * 6 + st[1][0] * 16 + st[1][1] * 12,
+                 alg["ab_bytes"]][dom]
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": world * 1000.0 / t_step, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded integrals and strings)",
+        "config": {"workload": args.workload, "determinants": n, "norb": ints.norb, "electrons": f"{ne}a/{ne}b",
+                   "strings_per_spin": ctx.na, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs (1.15 GB per vector) larger than L2; no flush"},
+        "e2e": {"value": world * 1000.0 / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": LAUNCHES_PER_SIGMA * args.steps * 2,
+        "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_kind,
+                     "traffic": args.traffic},
+        "phases_ms": {"alpha_same_spin_with_diag": parts[0] / args.steps,
+                      "beta_same_spin": parts[1] / args.steps, "alpha_beta": ab_ms},
+        "flops_per_sigma": alg["flops"], "fp64_tflops": alg["flops"] / (t_step * 1e-3) / 1e12,
+        "clocks": sampler.summary(),
+    }
+    if not args.no_cpu_baseline:
+        try:
+            rs = RefSampler(ints, ne, strs)
+            line["cpu_baseline"] = rs.sample(args.ref_budget)
+            rs.close()
+        except Exception as e:  # the reference checker may be absent on a fresh box
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    print(json.dumps(line))
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-budget", type=float, default=20.0, help="seconds of CPU work per reference sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the dominant kernel")
+    ap.add_argument("--workload", default=WORKLOAD, help="named workload (smaller ones for profiling captures)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

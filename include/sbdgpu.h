@@ -118,9 +118,14 @@ int sbdgpu_occupation(sbdgpu_ctx* ctx, const double* W, double* density);
  * carry-over selection (DiagonalReducedDensityMatrix, chemistry/tpb/rdmat.h:11-58). */
 int sbdgpu_alpha_weights(sbdgpu_ctx* ctx, const double* W, double* D);
 
-/* Device time in milliseconds of the kernels of the last sigma build, split
- * as [diagonal+alpha same-spin, beta same-spin incl. transposes, alpha-beta]. */
-int sbdgpu_last_sigma_ms(sbdgpu_ctx* ctx, float* ms3);
+/* CUDA-event times in milliseconds of the last sigma build, on the context's
+ * stream: ms5[0] diagonal + alpha same-spin kernel, [1] beta same-spin
+ * (transposes included), [2] alpha-beta kernel, [3] the whole build on device
+ * vectors (sign phases included), [4] for sbdgpu_sigma only: end to end from
+ * the start of the host-to-device copy to the end of the device-to-host copy
+ * (0 after a device-vector call).  No counterpart in the reference, which
+ * prints wall-clock timers (chemistry/tpb/mult.h:435-446, 619-646). */
+int sbdgpu_last_sigma_ms(sbdgpu_ctx* ctx, float* ms5);
 
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);
 void sbdgpu_destroy(sbdgpu_ctx* ctx);

@@ -133,7 +133,7 @@ class Context:
         self._check(lib().sbdgpu_sigma_device(self._h, _vp(dC_ptr), _vp(dS_ptr), precision))
 
     def last_sigma_ms(self):
-        a = (ctypes.c_float * 3)()
+        a = (ctypes.c_float * 5)()
         self._check(lib().sbdgpu_last_sigma_ms(self._h, a))
         return [float(x) for x in a]
 

@@ -119,13 +119,19 @@ void check_precision(int precision) {
 void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS) {
   // dC, dS in the reference (interleaved) sign convention
   ensure_io(c);
-  SBD_CUDA(cudaMemcpyAsync(c->io_a, dC, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
   sbdgpu::build_tables(c);
+  sbdgpu::compute_hii(c);
+  sbdgpu::ensure_scratch(c);
+  SBD_CUDA(cudaEventRecord(c->ev[4], c->stream));
+  SBD_CUDA(cudaMemcpyAsync(c->io_a, dC, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
   sbdgpu::apply_phase(c, c->io_a);
   sbdgpu::sigma_fp64(c, c->io_a, dS);
   sbdgpu::apply_phase(c, dS);
+  SBD_CUDA(cudaEventRecord(c->ev[5], c->stream));
   SBD_CUDA(cudaStreamSynchronize(c->stream));
   for (int k = 0; k < 3; k++) SBD_CUDA(cudaEventElapsedTime(&c->last_ms[k], c->ev[k], c->ev[k + 1]));
+  SBD_CUDA(cudaEventElapsedTime(&c->last_ms[3], c->ev[4], c->ev[5]));
+  c->last_ms[4] = 0.0f;
 }
 
 }  // namespace
@@ -163,7 +169,7 @@ int sbdgpu_create(sbdgpu_ctx** out, int norb, size_t na, size_t nb, const uint64
         c->h_vf[i * P + j] = eri_packed[a * (a + 1) / 2 + b];
       }
     SBD_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    for (int k = 0; k < 4; k++) SBD_CUDA(cudaEventCreate(&c->ev[k]));
+    for (int k = 0; k < 8; k++) SBD_CUDA(cudaEventCreate(&c->ev[k]));
     c->astr = (uint64_t*)sbdgpu::dev_alloc(sizeof(uint64_t) * na);
     c->bstr = (uint64_t*)sbdgpu::dev_alloc(sizeof(uint64_t) * nb);
     c->h1 = (double*)sbdgpu::dev_alloc(sizeof(double) * norb * norb);
@@ -234,11 +240,17 @@ int sbdgpu_sigma(sbdgpu_ctx* c, const double* C, double* S, int precision) {
     if (!C || !S) throw Error{SBDGPU_ERR_ARG, "null vector"};
     check_precision(precision);
     ensure_io(c);
+    sbdgpu::build_tables(c);
+    sbdgpu::compute_hii(c);
+    sbdgpu::ensure_scratch(c);
+    SBD_CUDA(cudaEventRecord(c->ev[6], c->stream));
     SBD_CUDA(cudaMemcpyAsync(c->io_b, C, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
     // sigma_ref_convention stages the input in io_a, so io_b can take the result
     sigma_ref_convention(c, c->io_b, c->io_b);
     SBD_CUDA(cudaMemcpyAsync(S, c->io_b, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    SBD_CUDA(cudaEventRecord(c->ev[7], c->stream));
     SBD_CUDA(cudaStreamSynchronize(c->stream));
+    SBD_CUDA(cudaEventElapsedTime(&c->last_ms[4], c->ev[6], c->ev[7]));
   });
 }
 
@@ -250,9 +262,9 @@ int sbdgpu_sigma_device(sbdgpu_ctx* c, const double* dC, double* dS, int precisi
   });
 }
 
-int sbdgpu_last_sigma_ms(sbdgpu_ctx* c, float* ms3) {
+int sbdgpu_last_sigma_ms(sbdgpu_ctx* c, float* ms5) {
   return guarded(c, [&] {
-    for (int k = 0; k < 3; k++) ms3[k] = c->last_ms[k];
+    for (int k = 0; k < 5; k++) ms5[k] = c->last_ms[k];
   });
 }
 
@@ -399,7 +411,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);
   cudaFree(c->hii); cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);
-  for (int k = 0; k < 4; k++)
+  for (int k = 0; k < 8; k++)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

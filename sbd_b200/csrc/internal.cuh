@@ -92,8 +92,10 @@ struct sbdgpu_ctx {
   double* ct = nullptr;    // transposed C   [nb][na]
   double* st = nullptr;    // transposed sigma part [nb][na]
   double* red = nullptr;   // reduction scratch
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  float last_ms[3] = {0, 0, 0};
+  // ev[0..3]: kernel phases of one sigma; ev[4]/ev[5]: whole sigma incl. sign
+  // phases; ev[6]/ev[7]: host-to-device copy start .. device-to-host copy end
+  cudaEvent_t ev[8] = {};
+  float last_ms[5] = {0, 0, 0, 0, 0};
   std::string err;
 };
 
