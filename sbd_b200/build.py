@@ -57,6 +57,23 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+DRIVER = os.path.join(HERE, "bin", "diag")
+
+
+def build_driver(force: bool = False) -> str:
+    """The sample driver (same flags as the reference sample) linked to libsbdgpu.so."""
+    lib = build_lib()
+    src = os.path.join(HERE, "samples", "diag.cc")
+    hdr = os.path.join(HERE, "include", "sbd_gpu", "tpb.h")
+    if not force and not _stale(DRIVER, [src, hdr, lib]):
+        return DRIVER
+    os.makedirs(os.path.dirname(DRIVER), exist_ok=True)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(HERE, "include"), "-I", os.path.join(ROOT, "include"),
+                    src, "-o", DRIVER, "-L", HERE, "-lsbdgpu", "-Wl,-rpath,$ORIGIN/.."], check=True)
+    return DRIVER
+
+
 if __name__ == "__main__":
     build_lib(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    build_driver(force="--force" in sys.argv)
+    print(LIB, DRIVER)
