@@ -92,6 +92,19 @@ int sbdgpu_sigma(sbdgpu_ctx* ctx, const double* C, double* sigma, int precision)
  * after it completes. */
 int sbdgpu_sigma_device(sbdgpu_ctx* ctx, const double* dC, double* dsigma, int precision);
 
+/* sigma = H*C with device vectors, for callers that cannot allocate device
+ * memory during the call (a pre-reserved memory pool or arena owns the
+ * device, or the call sits on a path that must not synchronise the device as
+ * cudaMalloc/cudaFree can).  No counterpart in the reference.  It allocates
+ * nothing: its scratch is one 12 MiB file-scope device array (3 x 524,288
+ * doubles) that every GPU loading this library holds until exit.  Limits:
+ * na*nb <= 524,288 (SBDGPU_ERR_LIMIT otherwise); the context's set-up must be
+ * done first (sbdgpu_build_tables and sbdgpu_diag, else SBDGPU_ERR_STATE); the
+ * first call on a device resolves the array's address and should come before
+ * any stream capture; all calls share the array, so calls that overlap on the
+ * GPU race.  Same result as sbdgpu_sigma_device, FP64 only. */
+int sbdgpu_sigma_device_noalloc(sbdgpu_ctx* ctx, const double* dC, double* dsigma);
+
 /* Restarted Davidson for the lowest root, the reference algorithm of
  * chemistry/tpb/davidson.h:661-923 (block <= max_nb, collapse restart,
  * diagonal preconditioner with eps_reg = 1e-12, modified Gram-Schmidt,

@@ -24,6 +24,7 @@ EXPORTS = [
     "sbdgpu_create", "sbdgpu_build_tables", "sbdgpu_table_sizes", "sbdgpu_get_tables", "sbdgpu_diag",
     "sbdgpu_sigma", "sbdgpu_sigma_device", "sbdgpu_davidson", "sbdgpu_rdm", "sbdgpu_occupation",
     "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
+    "sbdgpu_sigma_device_noalloc",
 ]
 
 
@@ -55,6 +56,7 @@ def lib():
         L.sbdgpu_diag.argtypes = [_vp, _dp]
         L.sbdgpu_sigma.argtypes = [_vp, _dp, _dp, ctypes.c_int]
         L.sbdgpu_sigma_device.argtypes = [_vp, _vp, _vp, ctypes.c_int]
+        L.sbdgpu_sigma_device_noalloc.argtypes = [_vp, _vp, _vp]
         L.sbdgpu_davidson.argtypes = [_vp, ctypes.POINTER(Opts), _dp, _dp, _dp, _dp, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
@@ -131,6 +133,12 @@ class Context:
 
     def sigma_device(self, dC_ptr: int, dS_ptr: int, precision: int = FP64) -> None:
         self._check(lib().sbdgpu_sigma_device(self._h, _vp(dC_ptr), _vp(dS_ptr), precision))
+
+    def sigma_device_noalloc(self, dC_ptr: int, dS_ptr: int) -> None:
+        """FP64 sigma on device vectors that allocates nothing during the call
+        (scratch in a fixed 12 MiB device array; at most 524,288 determinants;
+        the set-up, tables() and hii(), must have run first)."""
+        self._check(lib().sbdgpu_sigma_device_noalloc(self._h, _vp(dC_ptr), _vp(dS_ptr)))
 
     def last_sigma_ms(self):
         a = (ctypes.c_float * 5)()

@@ -124,6 +124,7 @@ void alpha_weights(sbdgpu_ctx* c, const double* dW, double* D);
 
 // sigma.cu
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);
+void sigma_fp64_prepared(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st);
 
 // api.cu
 void ensure_scratch(sbdgpu_ctx* c);

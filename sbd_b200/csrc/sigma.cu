@@ -205,4 +205,46 @@ void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S) {
   SBD_CUDA(cudaEventRecord(c->ev[3], st));
 }
 
+// The kernel sequence of sigma_fp64 on caller-provided scratch (ct, st: na*nb
+// doubles each).  Launches only: it allocates nothing and builds nothing, so
+// the tables, H_ii and the J tables must exist already.
+void sigma_fp64_prepared(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st) {
+  const SpinTables& ta = c->tab[0];
+  const SpinTables& tb = c->tab[1];
+  cudaStream_t s = c->stream;
+  {
+    dim3 g((unsigned)c->na, (unsigned)((c->nb + kRowsThreads * kRowsCols - 1) / (kRowsThreads * kRowsCols)));
+    rows_kernel<true><<<g, kRowsThreads, 0, s>>>(C, S, c->nb, c->hii, ta.s_off, ta.s_idx, ta.s_info, ta.s_val,
+                                                 ta.d_off, ta.d_idx, ta.d_val, c->jb);
+    SBD_CUDA(cudaGetLastError());
+  }
+  transpose(C, ct, c->na, c->nb, s);
+  {
+    dim3 g((unsigned)c->nb, (unsigned)((c->na + kRowsThreads * kRowsCols - 1) / (kRowsThreads * kRowsCols)));
+    rows_kernel<false><<<g, kRowsThreads, 0, s>>>(ct, st, c->na, nullptr, tb.s_off, tb.s_idx, tb.s_info, tb.s_val,
+                                                  tb.d_off, tb.d_idx, tb.d_val, c->ja);
+    SBD_CUDA(cudaGetLastError());
+  }
+  transpose_add(st, S, c->nb, c->na, s);
+  int dev_smem = 0;
+  SBD_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  size_t budget = (size_t)dev_smem - 1024;
+  size_t base = sizeof(double) * c->nb;
+  size_t per = sizeof(double) * c->P;
+  if (c->nb > 65536) throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: more than 65536 beta strings"};
+  if (base + per > budget)
+    throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: one FP64 beta row and integral row exceed shared memory"};
+  size_t gmax = (budget - base) / per;
+  if (gmax >= 16)
+    launch_ab<16>(c, C, S, base + 16 * per);
+  else if (gmax >= 8)
+    launch_ab<8>(c, C, S, base + 8 * per);
+  else if (gmax >= 4)
+    launch_ab<4>(c, C, S, base + 4 * per);
+  else if (gmax >= 2)
+    launch_ab<2>(c, C, S, base + 2 * per);
+  else
+    launch_ab<1>(c, C, S, base + per);
+}
+
 }  // namespace sbdgpu
