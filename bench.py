@@ -241,6 +241,32 @@ def run_reference(args):
     return 0
 
 
+def time_to_e0(ctx, args):
+    """Davidson from the aufbau determinant, plain FP64 against mixed precision.
+    The FP64 run goes to a tight residual; its final <W|HW> is the reference
+    energy.  Plain time-to-E0 = time of the first step whose Ritz value is
+    within 1e-6 Eh of it (steps cost the same: one sigma each); mixed
+    time-to-E0 = the whole mixed run including its FP64 refinement sigma, whose
+    energy must land within 1e-6 Eh."""
+    import sbd_b200
+    W0 = np.zeros(ctx.n)
+    W0[0] = 1.0
+    t = time.perf_counter()
+    e_ref, _, te, tt = ctx.davidson(W0, 100, 10, args.e0_tol, precision=sbd_b200.FP64)
+    t_plain_all = time.perf_counter() - t
+    hit = np.nonzero(te - e_ref < 1e-6)[0]
+    k = int(hit[0]) + 1 if len(hit) else len(te)
+    t_plain = t_plain_all * k / len(te)
+    t = time.perf_counter()
+    e_mix, _, tm, ttm = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED)
+    t_mixed = time.perf_counter() - t
+    return {"e_fp64": e_ref, "e_mixed": e_mix, "abs_err_mixed": abs(e_mix - e_ref),
+            "plain_steps_total": len(te), "plain_steps_to_1e-6": k, "plain_s_to_1e-6": t_plain,
+            "plain_final_residual": float(tt[-1]), "mixed_steps": len(tm), "mixed_s": t_mixed,
+            "mixed_final_residual": float(ttm[-1]), "speedup": t_plain / t_mixed,
+            "note": "wall-clock seconds (one sigma per step dominates); plain time prorated by steps"}
+
+
 def run_gpu(args):
     import torch
     import sbd_b200
@@ -278,6 +304,13 @@ def run_gpu(args):
         tot += ms[3]
         for k in range(3):
             parts[k] += ms[k]
+    torch.cuda.synchronize()
+    # the mixed-precision sigma (FP32 vectors) on the same resident vector
+    mixed_ms = []
+    for i in range(args.warmup + args.steps):
+        ctx.sigma_device(C.data_ptr(), S.data_ptr(), precision=sbd_b200.MIXED)
+        if i >= args.warmup:
+            mixed_ms.append(ctx.last_sigma_ms())
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
@@ -338,8 +371,13 @@ def run_gpu(args):
         "phases_ms": {"alpha_same_spin_with_diag": parts[0] / args.steps,
                       "beta_same_spin": parts[1] / args.steps, "alpha_beta": ab_ms},
         "flops_per_sigma": alg["flops"], "fp64_tflops": alg["flops"] / (t_step * 1e-3) / 1e12,
+        "mixed_fp32": {"sigma_per_s": 1000.0 * len(mixed_ms) / sum(m[3] for m in mixed_ms),
+                       "phases_ms": [sum(m[k] for m in mixed_ms) / len(mixed_ms) for k in range(3)],
+                       "note": "FP32 vectors and sigma incl. FP64<->FP32 conversion at the ABI"},
         "clocks": sampler.summary(),
     }
+    if args.time_to_e0:
+        line["time_to_e0"] = time_to_e0(ctx, args)
     if not args.no_cpu_baseline:
         try:
             rs = RefSampler(ints, ne, strs)
@@ -366,6 +404,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the dominant kernel")
     ap.add_argument("--workload", default=WORKLOAD, help="named workload (smaller ones for profiling captures)")
+    ap.add_argument("--time-to-e0", action="store_true", help="also time Davidson to E0 within 1e-6 Eh")
+    ap.add_argument("--e0-tol", type=float, default=1e-7, help="residual target of the FP64 reference run")
+    ap.add_argument("--mixed-tol", type=float, default=1e-4, help="residual target of the mixed run")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

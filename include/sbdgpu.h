@@ -42,7 +42,9 @@ typedef struct sbdgpu_ctx sbdgpu_ctx;
 #define SBDGPU_ERR_STATE 5
 
 /* Arithmetic of a sigma build. */
-#define SBDGPU_FP64 0 /* plain path: every product and sum in FP64 */
+#define SBDGPU_FP64 0  /* plain path: every product and sum in FP64 */
+#define SBDGPU_MIXED 1 /* FP32 vectors and FP32 sigma; FP64 dot products, Ritz
+                          step, residual norms and a final FP64 refinement sigma */
 
 /* Davidson options: the reference SBD fields that steer the solver
  * (chemistry/tpb/sbdiag.h:12-30). */
@@ -51,7 +53,7 @@ typedef struct sbdgpu_opts {
   int max_nb;       /* SBD::max_nb (--block), Krylov block <= 32 */
   double eps;       /* SBD::eps (--tolerance), residual-norm target */
   double max_time;  /* SBD::max_time, wall-time budget in seconds */
-  int precision;    /* SBDGPU_FP64 */
+  int precision;    /* SBDGPU_FP64 or SBDGPU_MIXED */
   int verbose;      /* 1: print the reference's "Davidson iteration" lines */
 } sbdgpu_opts;
 

@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsbdgpu.so")
 
 FP64 = 0
+MIXED = 1
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _dp = ctypes.POINTER(ctypes.c_double)

@@ -113,25 +113,126 @@ int guarded(sbdgpu_ctx* c, F&& f) {
 using sbdgpu::ensure_io;
 
 void check_precision(int precision) {
-  if (precision != SBDGPU_FP64) throw Error{SBDGPU_ERR_ARG, "unsupported precision " + std::to_string(precision)};
+  if (precision != SBDGPU_FP64 && precision != SBDGPU_MIXED)
+    throw Error{SBDGPU_ERR_ARG, "unsupported precision " + std::to_string(precision)};
 }
 
-void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS) {
+void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS, int precision = SBDGPU_FP64) {
   // dC, dS in the reference (interleaved) sign convention
   ensure_io(c);
   sbdgpu::build_tables(c);
   sbdgpu::compute_hii(c);
   sbdgpu::ensure_scratch(c);
+  if (precision == SBDGPU_MIXED) sbdgpu::ensure_fp32(c);
   SBD_CUDA(cudaEventRecord(c->ev[4], c->stream));
   SBD_CUDA(cudaMemcpyAsync(c->io_a, dC, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
   sbdgpu::apply_phase(c, c->io_a);
-  sbdgpu::sigma_fp64(c, c->io_a, dS);
+  if (precision == SBDGPU_MIXED) {
+    if (!c->io32) c->io32 = (float*)sbdgpu::dev_alloc(sizeof(float) * 2 * c->N);
+    float* c32 = c->io32;
+    float* s32 = c->io32 + c->N;
+    sbdgpu::convert(c->io_a, c32, c->N, c->stream);
+    sbdgpu::sigma_fp32(c, c32, s32);
+    sbdgpu::convert(s32, dS, c->N, c->stream);
+  } else {
+    sbdgpu::sigma_fp64(c, c->io_a, dS);
+  }
   sbdgpu::apply_phase(c, dS);
   SBD_CUDA(cudaEventRecord(c->ev[5], c->stream));
   SBD_CUDA(cudaStreamSynchronize(c->stream));
   for (int k = 0; k < 3; k++) SBD_CUDA(cudaEventElapsedTime(&c->last_ms[k], c->ev[k], c->ev[k + 1]));
   SBD_CUDA(cudaEventElapsedTime(&c->last_ms[3], c->ev[4], c->ev[5]));
   c->last_ms[4] = 0.0f;
+}
+
+// Mixed-precision Davidson: FP32 basis and FP32 sigma; FP64 dot products,
+// projected matrix, Ritz vector, residual, preconditioned correction and
+// Gram-Schmidt; the energy is the FP64 Rayleigh quotient <W|H W> from one FP64
+// refinement sigma of the final Ritz vector (the same final step as
+// chemistry/tpb/sbdiag.h:239-262).  Vectors in the alpha-string-major convention.
+void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, double* energy, double* trace_e,
+                    double* trace_tol, int max_trace, int* n_steps) {
+  int nb = o->max_nb;
+  size_t n = c->N;
+  cudaStream_t st = c->stream;
+  sbdgpu::ensure_fp32(c);
+  std::vector<float*> C(nb, nullptr), HC(nb, nullptr);
+  double* X = nullptr;  // FP64 correction vector
+  struct Free {
+    std::vector<float*>* a;
+    std::vector<float*>* b;
+    double** x;
+    ~Free() {
+      for (auto p : *a) cudaFree(p);
+      for (auto p : *b) cudaFree(p);
+      cudaFree(*x);
+    }
+  } guard{&C, &HC, &X};
+  for (int k = 0; k < nb; k++) {
+    C[k] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
+    HC[k] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
+  }
+  X = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+  const double eps_reg = 1.0e-12;
+  std::vector<double> H(nb * nb, 0.0), U(nb * nb, 0.0), E(nb, 0.0);
+  std::vector<double> step_times;
+  auto t_start = std::chrono::steady_clock::now();
+  int steps = 0;
+  bool cont = true;
+  for (int it = 0; it < o->max_it && cont; it++) {
+    sbdgpu::convert(W, C[0], n, st);
+    for (int ib = 0; ib < nb; ib++) {
+      auto t0 = std::chrono::steady_clock::now();
+      sbdgpu::sigma_fp32(c, C[ib], HC[ib]);
+      for (int jb = 0; jb <= ib; jb++) {
+        H[jb + nb * ib] = sbdgpu::dot_f(c, C[jb], nullptr, HC[ib], n);
+        H[ib + nb * jb] = H[jb + nb * ib];
+      }
+      for (int jb = 0; jb <= ib; jb++)
+        for (int kb = 0; kb <= ib; kb++) U[jb + nb * kb] = H[jb + nb * kb];
+      sbdgpu::jacobi_eig(ib + 1, U.data(), nb, E.data());
+      sbdgpu::ritz_update_f(C.data(), HC.data(), U.data(), ib + 1, E[0], W, R, n, c);
+      double nw = std::sqrt(sbdgpu::dot(c, W, W, n));
+      sbdgpu::scale(W, 1.0 / nw, n, st);
+      double tol = std::sqrt(sbdgpu::dot(c, R, R, n));
+      sbdgpu::scale(R, 1.0 / tol, n, st);
+      if (trace_e && steps < max_trace) trace_e[steps] = E[0];
+      if (trace_tol && steps < max_trace) trace_tol[steps] = tol;
+      steps++;
+      if (o->verbose) {
+        std::cout << " Davidson iteration " << it << "." << ib << " (tol=" << tol << "):";
+        for (int p = 0; p < std::min(ib + 1, 4); p++) std::cout << " " << E[p];
+        std::cout << std::endl;
+      }
+      if (tol < o->eps) {
+        cont = false;
+        break;
+      }
+      if (ib < nb - 1) {
+        sbdgpu::precondition(R, c->hii, E[0], eps_reg, X, n, st);
+        for (int kb = 0; kb < ib + 1; kb++) {
+          double olap = sbdgpu::dot_f(c, C[kb], X, C[kb], n);  // <X|C_kb> with X in FP64
+          sbdgpu::axpy_df(X, C[kb], -olap, n, st);
+        }
+        double nc = std::sqrt(sbdgpu::dot(c, X, X, n));
+        sbdgpu::scale(X, 1.0 / nc, n, st);
+        sbdgpu::convert(X, C[ib + 1], n, st);
+      }
+      SBD_CUDA(cudaStreamSynchronize(st));
+      auto t1 = std::chrono::steady_clock::now();
+      step_times.push_back(std::chrono::duration<double>(t1 - t0).count());
+      double avg = 0.0;
+      for (double x : step_times) avg += x;
+      avg /= step_times.size();
+      if (std::chrono::duration<double>(t1 - t_start).count() + avg > o->max_time) {
+        cont = false;
+        break;
+      }
+    }
+  }
+  sbdgpu::sigma_fp64(c, W, R);  // FP64 refinement sigma
+  *energy = sbdgpu::dot(c, W, R, n);
+  *n_steps = steps;
 }
 
 }  // namespace
@@ -246,7 +347,7 @@ int sbdgpu_sigma(sbdgpu_ctx* c, const double* C, double* S, int precision) {
     SBD_CUDA(cudaEventRecord(c->ev[6], c->stream));
     SBD_CUDA(cudaMemcpyAsync(c->io_b, C, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
     // sigma_ref_convention stages the input in io_a, so io_b can take the result
-    sigma_ref_convention(c, c->io_b, c->io_b);
+    sigma_ref_convention(c, c->io_b, c->io_b, precision);
     SBD_CUDA(cudaMemcpyAsync(S, c->io_b, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
     SBD_CUDA(cudaEventRecord(c->ev[7], c->stream));
     SBD_CUDA(cudaStreamSynchronize(c->stream));
@@ -258,7 +359,7 @@ int sbdgpu_sigma_device(sbdgpu_ctx* c, const double* dC, double* dS, int precisi
   return guarded(c, [&] {
     if (!dC || !dS) throw Error{SBDGPU_ERR_ARG, "null vector"};
     check_precision(precision);
-    sigma_ref_convention(c, dC, dS);
+    sigma_ref_convention(c, dC, dS, precision);
   });
 }
 
@@ -294,14 +395,25 @@ int sbdgpu_davidson(sbdgpu_ctx* c, const sbdgpu_opts* o, double* Wh, double* ene
         cudaFree(*r);
       }
     } guard{&C, &HC, &W, &R};
-    for (int k = 0; k < nb; k++) {
-      C[k] = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
-      HC[k] = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
-    }
     W = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
     R = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
     SBD_CUDA(cudaMemcpyAsync(W, Wh, sizeof(double) * n, cudaMemcpyHostToDevice, st));
     sbdgpu::apply_phase(c, W);
+    if (o->precision == SBDGPU_MIXED) {
+      double e = 0.0;
+      int steps = 0;
+      davidson_mixed(c, o, W, R, &e, trace_e, trace_tol, max_trace, &steps);
+      sbdgpu::apply_phase(c, W);
+      SBD_CUDA(cudaMemcpyAsync(Wh, W, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+      SBD_CUDA(cudaStreamSynchronize(st));
+      if (energy) *energy = e;
+      if (n_steps) *n_steps = steps;
+      return;
+    }
+    for (int k = 0; k < nb; k++) {
+      C[k] = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+      HC[k] = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+    }
     const double eps_reg = 1.0e-12;
     std::vector<double> H(nb * nb, 0.0), U(nb * nb, 0.0), E(nb, 0.0);
     std::vector<double> step_times;
@@ -410,7 +522,8 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);
-  cudaFree(c->hii); cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);
+  cudaFree(c->hii); cudaFree(c->io32); cudaFree(c->ja32); cudaFree(c->jb32); cudaFree(c->vf32);
+  cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);
   for (int k = 0; k < 8; k++)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   if (c->stream) cudaStreamDestroy(c->stream);

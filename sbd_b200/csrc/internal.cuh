@@ -83,12 +83,16 @@ struct sbdgpu_ctx {
   double* ja = nullptr;  // [P][na]
   double* jb = nullptr;  // [P][nb]
   double* hii = nullptr; // [N]
+  float* ja32 = nullptr; // FP32 copies for the mixed path
+  float* jb32 = nullptr;
+  float* vf32 = nullptr;
   sbdgpu::SpinTables tab[2];
   bool tables_ready = false;
   bool hii_ready = false;
   // scratch vectors (FP64, N each), allocated on first use
   double* io_a = nullptr;  // user I/O staging
   double* io_b = nullptr;
+  float* io32 = nullptr;   // FP32 staging of C and sigma (mixed path), 2*N
   double* ct = nullptr;    // transposed C   [nb][na]
   double* st = nullptr;    // transposed sigma part [nb][na]
   double* red = nullptr;   // reduction scratch
@@ -109,10 +113,19 @@ void free_tables(SpinTables& t);
 void build_j_tables(sbdgpu_ctx* c);
 void compute_hii(sbdgpu_ctx* c);
 void apply_phase(sbdgpu_ctx* c, double* v);
-void transpose(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s);
-void transpose_add(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s);
+template <typename T>
+void transpose(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s);
+template <typename T>
+void transpose_add(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s);
+void ensure_fp32(sbdgpu_ctx* c);
 double dot(sbdgpu_ctx* c, const double* x, const double* y, size_t n);
 void scale(double* x, double a, size_t n, cudaStream_t s);
+double dot_f(sbdgpu_ctx* c, const float* x, const double* xd, const float* y, size_t n);
+void axpy_df(double* y, const float* x, double a, size_t n, cudaStream_t s);
+void convert(const double* in, float* out, size_t n, cudaStream_t s);
+void convert(const float* in, double* out, size_t n, cudaStream_t s);
+void ritz_update_f(float* const* C, float* const* HC, const double* U, int nk, double e0, double* W, double* R,
+                   size_t n, sbdgpu_ctx* c);
 void axpy(double* y, const double* x, double a, size_t n, cudaStream_t s);
 void ritz_update(double* const* C, double* const* HC, const double* U, int nk, double e0, double* W,
                  double* R, size_t n, cudaStream_t s);
@@ -125,6 +138,7 @@ void alpha_weights(sbdgpu_ctx* c, const double* dW, double* D);
 // sigma.cu
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);
 void sigma_fp64_prepared(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st);
+void sigma_fp32(sbdgpu_ctx* c, const float* C, float* S);
 
 // api.cu
 void ensure_scratch(sbdgpu_ctx* c);

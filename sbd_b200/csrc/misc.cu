@@ -83,10 +83,9 @@ __global__ void phase_kernel(const uint64_t* __restrict__ astr, const uint64_t* 
   if (cnt & 1) v[ia * nb + ib] = -v[ia * nb + ib];
 }
 
-template <bool kAdd>
-__global__ void transpose_kernel(const double* __restrict__ in, double* __restrict__ out, size_t rows,
-                                 size_t cols) {
-  __shared__ double tile[32][33];
+template <typename T, bool kAdd>
+__global__ void transpose_kernel(const T* __restrict__ in, T* __restrict__ out, size_t rows, size_t cols) {
+  __shared__ T tile[32][33];
   size_t c0 = (size_t)blockIdx.x * 32, r0 = (size_t)blockIdx.y * 32;
   int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   for (int k = ty; k < 32; k += 8) {
@@ -143,6 +142,55 @@ __global__ void scale_kernel(double* x, double a, size_t n) {
 __global__ void axpy_kernel(double* y, const double* x, double a, size_t n) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     y[i] += x[i] * a;
+}
+
+__global__ void dot_partial_f(const float* __restrict__ x, const float* __restrict__ y, const double* __restrict__ xd,
+                              size_t n, double* __restrict__ part) {
+  __shared__ double sh[kRedThreads / 32];
+  double acc = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    acc += (xd ? xd[i] : (double)x[i]) * (double)y[i];
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kRedThreads / 32; w++) s += sh[w];
+    part[blockIdx.x] = s;
+  }
+}
+
+__global__ void axpy_df_kernel(double* y, const float* x, double a, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] += (double)x[i] * a;
+}
+
+__global__ void convert_kernel_df(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+__global__ void convert_kernel_fd(const float* __restrict__ in, double* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+struct PtrPackF {
+  const float* p[32];
+};
+
+// mixed path: W = sum_k U_k C_k ; R = E0*W - sum_k U_k HC_k, FP32 basis, FP64 result
+__global__ void ritz_kernel_f(PtrPackF c, PtrPackF hc, const double* __restrict__ u, int nk, double e0,
+                              double* __restrict__ W, double* __restrict__ R, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double w = 0.0, r = 0.0;
+    for (int k = 0; k < nk; k++) {
+      w += (double)c.p[k][i] * u[k];
+      r -= (double)hc.p[k][i] * u[k];
+    }
+    W[i] = w;
+    R[i] = r + e0 * w;
+  }
 }
 
 struct PtrPack {
@@ -398,15 +446,40 @@ void apply_phase(sbdgpu_ctx* c, double* v) {
   SBD_CUDA(cudaGetLastError());
 }
 
-void transpose(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s) {
+template <typename T>
+void transpose(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s) {
   dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
-  transpose_kernel<false><<<g, dim3(32, 8), 0, s>>>(in, out, rows, cols);
+  transpose_kernel<T, false><<<g, dim3(32, 8), 0, s>>>(in, out, rows, cols);
   SBD_CUDA(cudaGetLastError());
 }
 
-void transpose_add(const double* in, double* out, size_t rows, size_t cols, cudaStream_t s) {
+template <typename T>
+void transpose_add(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s) {
   dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
-  transpose_kernel<true><<<g, dim3(32, 8), 0, s>>>(in, out, rows, cols);
+  transpose_kernel<T, true><<<g, dim3(32, 8), 0, s>>>(in, out, rows, cols);
+  SBD_CUDA(cudaGetLastError());
+}
+
+template void transpose<double>(const double*, double*, size_t, size_t, cudaStream_t);
+template void transpose<float>(const float*, float*, size_t, size_t, cudaStream_t);
+template void transpose_add<double>(const double*, double*, size_t, size_t, cudaStream_t);
+template void transpose_add<float>(const float*, float*, size_t, size_t, cudaStream_t);
+
+__global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+void ensure_fp32(sbdgpu_ctx* c) {
+  if (c->vf32) return;
+  build_j_tables(c);
+  size_t nja = (size_t)c->P * c->na, njb = (size_t)c->P * c->nb, nvf = (size_t)c->P * c->P;
+  c->ja32 = (float*)dev_alloc(sizeof(float) * nja);
+  c->jb32 = (float*)dev_alloc(sizeof(float) * njb);
+  c->vf32 = (float*)dev_alloc(sizeof(float) * nvf);
+  to_float_kernel<<<592, 256, 0, c->stream>>>(c->ja, c->ja32, nja);
+  to_float_kernel<<<592, 256, 0, c->stream>>>(c->jb, c->jb32, njb);
+  to_float_kernel<<<592, 256, 0, c->stream>>>(c->vf, c->vf32, nvf);
   SBD_CUDA(cudaGetLastError());
 }
 
@@ -419,6 +492,47 @@ double dot(sbdgpu_ctx* c, const double* x, const double* y, size_t n) {
   SBD_CUDA(cudaMemcpyAsync(&r, c->red + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SBD_CUDA(cudaStreamSynchronize(c->stream));
   return r;
+}
+
+double dot_f(sbdgpu_ctx* c, const float* x, const double* xd, const float* y, size_t n) {
+  ensure_scratch(c);
+  dot_partial_f<<<kRedBlocks, kRedThreads, 0, c->stream>>>(x, y, xd, n, c->red);
+  dot_final<<<1, 1024, 0, c->stream>>>(c->red, kRedBlocks, c->red + kRedBlocks);
+  SBD_CUDA(cudaGetLastError());
+  double r = 0.0;
+  SBD_CUDA(cudaMemcpyAsync(&r, c->red + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+  return r;
+}
+
+void axpy_df(double* y, const float* x, double a, size_t n, cudaStream_t s) {
+  axpy_df_kernel<<<grid_for(n), 256, 0, s>>>(y, x, a, n);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void convert(const double* in, float* out, size_t n, cudaStream_t s) {
+  convert_kernel_df<<<grid_for(n), 256, 0, s>>>(in, out, n);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void convert(const float* in, double* out, size_t n, cudaStream_t s) {
+  convert_kernel_fd<<<grid_for(n), 256, 0, s>>>(in, out, n);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void ritz_update_f(float* const* C, float* const* HC, const double* U, int nk, double e0, double* W, double* R,
+                   size_t n, sbdgpu_ctx* c) {
+  PtrPackF pc{}, ph{};
+  for (int k = 0; k < nk; k++) {
+    pc.p[k] = C[k];
+    ph.p[k] = HC[k];
+  }
+  ensure_scratch(c);
+  double* du = c->red + 600;  // 32 spare doubles after the 593 reduction slots
+  SBD_CUDA(cudaMemcpyAsync(du, U, sizeof(double) * nk, cudaMemcpyHostToDevice, c->stream));
+  ritz_kernel_f<<<grid_for(n), 256, 0, c->stream>>>(pc, ph, du, nk, e0, W, R, n);
+  SBD_CUDA(cudaGetLastError());
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
 }
 
 void scale(double* x, double a, size_t n, cudaStream_t s) {

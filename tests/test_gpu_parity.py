@@ -162,6 +162,8 @@ def test_invalid_inputs_rejected():
     with pytest.raises(sbd_b200.SbdGpuError):
         ctx.sigma(np.ones(4), precision=99)
     with pytest.raises(sbd_b200.SbdGpuError):
+        ctx.davidson(np.ones(4), 1, 8, 1e-8, precision=7)
+    with pytest.raises(sbd_b200.SbdGpuError):
         ctx.davidson(np.ones(4), 1, 64, 1e-8)
 
 
