@@ -84,36 +84,78 @@ __global__ void __launch_bounds__(kRowsThreads) rows_kernel(
 
 constexpr int kAbThreads = 512;
 
-// One CTA per (source alpha string ja, group of G of its singles).
+// Row stride (elements) of the integral block in shared memory: G values per
+// beta pair index rs, padded by 16 bytes so that the 16-byte vector loads of a
+// warp (random rs per lane) spread over 8 different 4-bank windows.
+template <typename T, int G>
+__host__ __device__ constexpr int ab_vstride() {
+  return G * (int)sizeof(T) >= 16 ? G + 16 / (int)sizeof(T) : G;
+}
+
+template <typename T, int G>
+__device__ __forceinline__ void ab_accumulate(const T* __restrict__ vr, T x, T (&y)[G]) {
+  if constexpr (G * sizeof(T) >= 16) {
+    constexpr int W = 16 / sizeof(T);
+#pragma unroll
+    for (int g = 0; g < G; g += W) {
+      if constexpr (sizeof(T) == 4) {
+        float4 v = *reinterpret_cast<const float4*>(vr + g);
+        y[g] += v.x * x;
+        y[g + 1] += v.y * x;
+        y[g + 2] += v.z * x;
+        y[g + 3] += v.w * x;
+      } else {
+        double2 v = *reinterpret_cast<const double2*>(vr + g);
+        y[g] += v.x * x;
+        y[g + 1] += v.y * x;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int g = 0; g < G; g++) y[g] += vr[g] * x;
+  }
+}
+
+// One CTA per (source alpha string ja, group of G of its singles).  Shared
+// memory: the source row C[ja,:] and, for every folded beta pair index rs, the
+// G integrals (pq_g|rs) of the group's alpha singles, contiguous.
 template <typename T, int G>
 __global__ void __launch_bounds__(kAbThreads) ab_kernel(
     const T* __restrict__ C, T* __restrict__ S, size_t nb, int P, const T* __restrict__ vf,
     const int64_t* __restrict__ a_off, const int32_t* __restrict__ a_idx, const uint32_t* __restrict__ a_info,
     const int64_t* __restrict__ sell_off, const int32_t* __restrict__ sell_w, const uint32_t* __restrict__ sell,
     size_t nslice) {
+  constexpr int VS = ab_vstride<T, G>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* crow = reinterpret_cast<T*>(smem_raw);  // [nb]
-  T* vsub = crow + nb;                       // [G][P]
+  T* crow = reinterpret_cast<T*>(smem_raw);  // [nb], padded to 16 bytes
+  T* vsub = reinterpret_cast<T*>(smem_raw + ((nb * sizeof(T) + 15) & ~size_t(15)));  // [P][VS]
   __shared__ int tgt[G];
   __shared__ T sgn[G];
+  __shared__ int pqs[G];
   size_t ja = blockIdx.x;
   int64_t k0 = a_off[ja] + (int64_t)blockIdx.y * G;
   int64_t k1 = min(k0 + G, a_off[ja + 1]);
   if (k0 >= k1) return;
   int gcount = (int)(k1 - k0);
-  for (size_t i = threadIdx.x; i < nb; i += blockDim.x) crow[i] = C[ja * nb + i];
-  for (int g = 0; g < G; g++) {
+  if (threadIdx.x < G) {
+    int g = threadIdx.x;
     if (g < gcount) {
       uint32_t info = a_info[k0 + g];
-      int pq = (info >> 12) & 0xFFFu;
-      for (int i = threadIdx.x; i < P; i += blockDim.x) vsub[g * P + i] = vf[(size_t)pq * P + i];
-      if (threadIdx.x == 0) {
-        tgt[g] = a_idx[k0 + g];
-        sgn[g] = (info & 0x80000000u) ? (T)-1 : (T)1;
-      }
+      pqs[g] = (info >> 12) & 0xFFFu;
+      tgt[g] = a_idx[k0 + g];
+      sgn[g] = (info & 0x80000000u) ? (T)-1 : (T)1;
     } else {
-      for (int i = threadIdx.x; i < P; i += blockDim.x) vsub[g * P + i] = (T)0;
+      pqs[g] = -1;
+      tgt[g] = 0;
+      sgn[g] = (T)0;
     }
+  }
+  for (size_t i = threadIdx.x; i < nb; i += blockDim.x) crow[i] = C[ja * nb + i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < P * G; i += blockDim.x) {
+    int g = i / P, rs = i - g * P;  // consecutive threads read consecutive rs of one integral row
+    int pq = pqs[g];
+    vsub[rs * VS + g] = pq >= 0 ? vf[(size_t)pq * P + rs] : (T)0;
   }
   __syncthreads();
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
@@ -129,9 +171,7 @@ __global__ void __launch_bounds__(kAbThreads) ab_kernel(
       if (e == kSellInvalid) continue;
       T x = crow[e & 0xFFFFu];
       if (e & 0x80000000u) x = -x;
-      const T* vr = vsub + ((e >> 16) & 0xFFFu);
-#pragma unroll
-      for (int g = 0; g < G; g++) y[g] += vr[g * P] * x;
+      ab_accumulate<T, G>(vsub + ((e >> 16) & 0xFFFu) * VS, x, y);
     }
     if (ib < nb) {
 #pragma unroll
@@ -139,6 +179,11 @@ __global__ void __launch_bounds__(kAbThreads) ab_kernel(
         if (g < gcount) atomicAdd(&S[(size_t)tgt[g] * nb + ib], sgn[g] * y[g]);
     }
   }
+}
+
+template <typename T, int G>
+size_t ab_smem(size_t nb, int P) {
+  return ((nb * sizeof(T) + 15) & ~size_t(15)) + (size_t)P * ab_vstride<T, G>() * sizeof(T);
 }
 
 template <typename T, int G>
@@ -180,22 +225,21 @@ void sigma_launch(sbdgpu_ctx* c, const T* C, T* S, T* ct, T* st, const T* ja, co
   int dev_smem = 0;
   SBD_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
   size_t budget = (size_t)dev_smem - 1024;
-  size_t base = sizeof(T) * c->nb;
-  size_t per = sizeof(T) * c->P;
   if (c->nb > 65536) throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: more than 65536 beta strings"};
-  if (base + per > budget)
-    throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: one beta row and integral row exceed shared memory"};
-  size_t gmax = (budget - base) / per;
-  if (gmax >= 16)
-    launch_ab<T, 16>(c, C, S, vf, base + 16 * per);
-  else if (gmax >= 8)
-    launch_ab<T, 8>(c, C, S, vf, base + 8 * per);
-  else if (gmax >= 4)
-    launch_ab<T, 4>(c, C, S, vf, base + 4 * per);
-  else if (gmax >= 2)
-    launch_ab<T, 2>(c, C, S, vf, base + 2 * per);
+  size_t nb = c->nb;
+  int P = c->P;
+  if (ab_smem<T, 16>(nb, P) <= budget)
+    launch_ab<T, 16>(c, C, S, vf, ab_smem<T, 16>(nb, P));
+  else if (ab_smem<T, 8>(nb, P) <= budget)
+    launch_ab<T, 8>(c, C, S, vf, ab_smem<T, 8>(nb, P));
+  else if (ab_smem<T, 4>(nb, P) <= budget)
+    launch_ab<T, 4>(c, C, S, vf, ab_smem<T, 4>(nb, P));
+  else if (ab_smem<T, 2>(nb, P) <= budget)
+    launch_ab<T, 2>(c, C, S, vf, ab_smem<T, 2>(nb, P));
+  else if (ab_smem<T, 1>(nb, P) <= budget)
+    launch_ab<T, 1>(c, C, S, vf, ab_smem<T, 1>(nb, P));
   else
-    launch_ab<T, 1>(c, C, S, vf, base + per);
+    throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: one beta row and integral row exceed shared memory"};
   if (events) SBD_CUDA(cudaEventRecord(c->ev[3], s));
 }
 
