@@ -22,85 +22,91 @@ namespace sbdgpu {
 
 namespace {
 
-constexpr int kBlockThreads = 256;
+constexpr int kBlockThreads = 256;  // 8 warps
+constexpr int kWarps = kBlockThreads / 32;
+constexpr int kSliceCols = 256;    // columns of C per CTA
+constexpr int kColsPerLane = kSliceCols / 32;
 
-template <typename T, bool kWithDiag, int R, int CPT>
+// CTA = (block of R bra rows, slice of 256 columns).  Warp w owns the block's
+// rows w, w+8, w+16, ...; lane l owns columns l, l+32, ..., so every entry
+// (warp-uniform) feeds 8 FMAs per lane from conflict-free shared memory.
+template <typename T, bool kWithDiag, int R>
 __global__ void __launch_bounds__(kBlockThreads, 2) block_rows_kernel(
     const T* __restrict__ C, T* __restrict__ S, size_t nrows, size_t ncols, const double* __restrict__ hii,
     const int64_t* __restrict__ blk_batch0, const int32_t* __restrict__ kets, const int64_t* __restrict__ eoff,
     const RowEntry* __restrict__ ent, const T* __restrict__ J) {
+  constexpr int RW = R / kWarps;  // rows per warp
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sm = reinterpret_cast<T*>(smem_raw);  // [kRowBatch][kBlockThreads * CPT]
-  constexpr int W = kBlockThreads * CPT;
+  T* sm = reinterpret_cast<T*>(smem_raw);  // [kRowBatch][kSliceCols]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const size_t b = blockIdx.x;
   const size_t row0 = b * R;
-  const size_t cbase = (size_t)blockIdx.y * W + threadIdx.x;
-  T acc[R][CPT];
+  const size_t cbase = (size_t)blockIdx.y * kSliceCols;
+  T acc[RW][kColsPerLane];
 #pragma unroll
-  for (int r = 0; r < R; r++)
+  for (int i = 0; i < RW; i++) {
+    size_t row = row0 + warp + (size_t)i * kWarps;
 #pragma unroll
-    for (int u = 0; u < CPT; u++) {
-      size_t row = row0 + r, col = cbase + (size_t)u * kBlockThreads;
-      acc[r][u] = (kWithDiag && row < nrows && col < ncols) ? (T)hii[row * ncols + col] * C[row * ncols + col]
+    for (int k = 0; k < kColsPerLane; k++) {
+      size_t col = cbase + lane + 32 * k;
+      acc[i][k] = (kWithDiag && row < nrows && col < ncols) ? (T)hii[row * ncols + col] * C[row * ncols + col]
                                                            : (T)0;
     }
+  }
   const int64_t g0 = blk_batch0[b], g1 = blk_batch0[b + 1];
   for (int64_t g = g0; g < g1; g++) {
     __syncthreads();
-#pragma unroll 4
-    for (int slot = 0; slot < kRowBatch; slot++) {
+    for (int idx = threadIdx.x; idx < kRowBatch * kSliceCols; idx += kBlockThreads) {
+      int slot = idx / kSliceCols, cc = idx - slot * kSliceCols;
       int ket = __ldg(&kets[g * kRowBatch + slot]);
-#pragma unroll
-      for (int u = 0; u < CPT; u++) {
-        size_t col = cbase + (size_t)u * kBlockThreads;
-        sm[slot * W + threadIdx.x + u * kBlockThreads] =
-            (ket >= 0 && col < ncols) ? C[(size_t)ket * ncols + col] : (T)0;
-      }
+      size_t col = cbase + cc;
+      sm[idx] = (ket >= 0 && col < ncols) ? C[(size_t)ket * ncols + col] : (T)0;
     }
     __syncthreads();
     const int64_t* eo = eoff + g * R;
 #pragma unroll
-    for (int r = 0; r < R; r++) {
+    for (int i = 0; i < RW; i++) {
+      const int r = warp + i * kWarps;
       const int64_t e0 = eo[r], e1 = eo[r + 1];
       for (int64_t e = e0; e < e1; e++) {
         RowEntry en = ent[e];
-        int slot = en.info & 0xFFu;
+        const T* x = sm + (en.info & 0xFFu) * kSliceCols + lane;
         T v = (T)en.val;
-        const T* x = sm + slot * W + threadIdx.x;
         if (en.info & 0x100u) {
-          const T* Jr = J + (size_t)((en.info >> 12) & 0xFFFu) * ncols;
+          const T* Jr = J + (size_t)((en.info >> 12) & 0xFFFu) * ncols + cbase + lane;
           T sg = (en.info & 0x80000000u) ? (T)-1 : (T)1;
 #pragma unroll
-          for (int u = 0; u < CPT; u++) {
-            size_t col = cbase + (size_t)u * kBlockThreads;
-            T jv = col < ncols ? Jr[col] : (T)0;
-            acc[r][u] += (v + sg * jv) * x[u * kBlockThreads];
+          for (int k = 0; k < kColsPerLane; k++) {
+            T jv = (cbase + lane + 32 * k < ncols) ? Jr[32 * k] : (T)0;
+            acc[i][k] += (v + sg * jv) * x[32 * k];
           }
         } else {
 #pragma unroll
-          for (int u = 0; u < CPT; u++) acc[r][u] += v * x[u * kBlockThreads];
+          for (int k = 0; k < kColsPerLane; k++) acc[i][k] += v * x[32 * k];
         }
       }
     }
   }
 #pragma unroll
-  for (int r = 0; r < R; r++)
+  for (int i = 0; i < RW; i++) {
+    size_t row = row0 + warp + (size_t)i * kWarps;
 #pragma unroll
-    for (int u = 0; u < CPT; u++) {
-      size_t row = row0 + r, col = cbase + (size_t)u * kBlockThreads;
-      if (row < nrows && col < ncols) S[row * ncols + col] = acc[r][u];
+    for (int k = 0; k < kColsPerLane; k++) {
+      size_t col = cbase + lane + 32 * k;
+      if (row < nrows && col < ncols) S[row * ncols + col] = acc[i][k];
     }
+  }
 }
 
-template <typename T, bool kWithDiag, int R, int CPT>
+template <typename T, bool kWithDiag, int R>
 void launch_block_rows(const RowBlocks& rb, const T* C, T* S, size_t nrows, size_t ncols, const double* hii,
                        const T* J, cudaStream_t s) {
-  size_t smem = sizeof(T) * kRowBatch * kBlockThreads * CPT;
-  SBD_CUDA(cudaFuncSetAttribute(block_rows_kernel<T, kWithDiag, R, CPT>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 g((unsigned)rb.nblk, (unsigned)((ncols + kBlockThreads * CPT - 1) / (kBlockThreads * CPT)));
-  block_rows_kernel<T, kWithDiag, R, CPT><<<g, kBlockThreads, smem, s>>>(C, S, nrows, ncols, hii, rb.blk_batch0,
-                                                                         rb.kets, rb.eoff, rb.ent, J);
+  size_t smem = sizeof(T) * kRowBatch * kSliceCols;
+  SBD_CUDA(cudaFuncSetAttribute(block_rows_kernel<T, kWithDiag, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+  dim3 g((unsigned)rb.nblk, (unsigned)((ncols + kSliceCols - 1) / kSliceCols));
+  block_rows_kernel<T, kWithDiag, R><<<g, kBlockThreads, smem, s>>>(C, S, nrows, ncols, hii, rb.blk_batch0,
+                                                                    rb.kets, rb.eoff, rb.ent, J);
   SBD_CUDA(cudaGetLastError());
 }
 
@@ -201,11 +207,7 @@ void free_row_blocks(RowBlocks& rb) {
 template <typename T, bool kWithDiag>
 void same_spin_blocked(const RowBlocks& rb, const T* C, T* S, size_t nrows, size_t ncols, const double* hii,
                        const T* J, cudaStream_t s) {
-  // FP64: one column per thread keeps the 32 x 1 accumulators at 64 registers
-  if constexpr (sizeof(T) == 8)
-    launch_block_rows<T, kWithDiag, kRowBlock, 1>(rb, C, S, nrows, ncols, hii, J, s);
-  else
-    launch_block_rows<T, kWithDiag, kRowBlock, 2>(rb, C, S, nrows, ncols, hii, J, s);
+  launch_block_rows<T, kWithDiag, kRowBlock>(rb, C, S, nrows, ncols, hii, J, s);
 }
 
 template void same_spin_blocked<double, true>(const RowBlocks&, const double*, double*, size_t, size_t,
