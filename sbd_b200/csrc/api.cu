@@ -521,8 +521,6 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
-  sbdgpu::free_row_blocks(c->blocks[0]);
-  sbdgpu::free_row_blocks(c->blocks[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);
   cudaFree(c->hii); cudaFree(c->io32); cudaFree(c->ja32); cudaFree(c->jb32); cudaFree(c->vf32);
   cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);

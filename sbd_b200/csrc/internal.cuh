@@ -60,26 +60,6 @@ struct SpinTables {
   std::vector<int64_t> h_s_off, h_d_off;  // host copies of the offsets
 };
 
-// Row blocks of the same-spin tables (see blocks.cu).
-constexpr int kRowBlock = 32;  // bra rows per block
-constexpr int kRowBatch = 16;  // ket rows staged in shared memory at a time
-
-struct RowEntry {
-  double val;     // matrix element (string-only part)
-  uint32_t info;  // slot (0..15) | single<<8 | pair<<12 | neg<<31
-  uint32_t pad;
-};
-
-struct RowBlocks {
-  int R = 0;
-  size_t nblk = 0;
-  int64_t nbatch = 0;
-  int64_t* blk_batch0 = nullptr;  // [nblk+1] first batch of each block
-  int32_t* kets = nullptr;        // [nbatch*kRowBatch], -1 = padding
-  int64_t* eoff = nullptr;        // [nbatch*R+1] entries of (batch, row)
-  RowEntry* ent = nullptr;
-};
-
 }  // namespace sbdgpu
 
 struct sbdgpu_ctx {
@@ -102,7 +82,6 @@ struct sbdgpu_ctx {
   float* jb32 = nullptr;
   float* vf32 = nullptr;
   sbdgpu::SpinTables tab[2];
-  sbdgpu::RowBlocks blocks[2];
   bool tables_ready = false;
   bool hii_ready = false;
   // scratch vectors (FP64, N each), allocated on first use
@@ -124,13 +103,6 @@ namespace sbdgpu {
 // tables.cu
 void build_tables(sbdgpu_ctx* c);
 void free_tables(SpinTables& t);
-
-// blocks.cu
-void build_row_blocks(sbdgpu_ctx* c, int spin, int R);
-void free_row_blocks(RowBlocks& rb);
-template <typename T, bool kWithDiag>
-void same_spin_blocked(const RowBlocks& rb, const T* C, T* S, size_t nrows, size_t ncols, const double* hii,
-                       const T* J, cudaStream_t s);
 
 // misc.cu
 void build_j_tables(sbdgpu_ctx* c);

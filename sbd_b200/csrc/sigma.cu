@@ -8,14 +8,14 @@
 //
 //  same-spin (alpha)     sigma[ia,:]  = hii[ia,:] C[ia,:] + sum_{ja in D(ia)} d C[ja,:]
 //                                       + sum_{ja in S(ia)} s (F + Jb_pq[:]) C[ja,:]
-//                        (task type 2 of the reference: alpha singles/doubles;
-//                        blocked over bra rows, blocks.cu)
+//                        (task type 2 of the reference: alpha singles/doubles)
 //  same-spin (beta)      the same kernel on the transposed vector C^T, with the
 //                        beta tables and Ja (task type 1), added back transposed
 //  alpha-beta kernel     sigma[ia,ib] += sum_{ja in S(ia)} sum_{jb in S(ib)}
 //                                        s_a s_b (pq|rs) C[ja,jb]   (task type 0)
 //
-// The alpha-beta kernel holds one source row C[ja,:] and the
+// The rows kernel streams whole rows of C (coalesced) for every table entry of
+// its bra row.  The alpha-beta kernel holds one source row C[ja,:] and the
 // integral rows (pq|.) of a group of ja's singles in shared memory, streams the
 // beta singles (sliced ELL, coalesced) once per group, and adds each group's
 // contributions to sigma rows ia with FP64 atomics.
@@ -26,6 +26,62 @@
 namespace sbdgpu {
 
 namespace {
+
+constexpr int kRowsThreads = 256;
+constexpr int kRowsCols = 2;  // columns per thread
+
+// sigma_row[ia][cols] (=) diag + sum over the bra's table entries, in the
+// vector type T (double: plain path; float: mixed path, FP32 accumulation).
+// J: [P][ncols] Coulomb coupling to the other spin's occupation.
+template <typename T, bool kWithDiag>
+__global__ void __launch_bounds__(kRowsThreads) rows_kernel(
+    const T* __restrict__ C, T* __restrict__ S, size_t ncols, const double* __restrict__ hii,
+    const int64_t* __restrict__ s_off, const int32_t* __restrict__ s_idx, const uint32_t* __restrict__ s_info,
+    const double* __restrict__ s_val, const int64_t* __restrict__ d_off, const int32_t* __restrict__ d_idx,
+    const double* __restrict__ d_val, const T* __restrict__ J) {
+  size_t row = blockIdx.x;
+  size_t c0 = (size_t)blockIdx.y * (kRowsThreads * kRowsCols) + threadIdx.x;
+  T acc[kRowsCols];
+  bool ok[kRowsCols];
+#pragma unroll
+  for (int u = 0; u < kRowsCols; u++) {
+    size_t col = c0 + (size_t)u * kRowsThreads;
+    ok[u] = col < ncols;
+    acc[u] = (kWithDiag && ok[u]) ? (T)hii[row * ncols + col] * C[row * ncols + col] : (T)0;
+  }
+  int64_t b = s_off[row], e = s_off[row + 1];
+  for (int64_t k = b; k < e; k++) {
+    size_t j = (size_t)__ldg(&s_idx[k]);
+    uint32_t info = __ldg(&s_info[k]);
+    T v = (T)__ldg(&s_val[k]);
+    T sg = (info & 0x80000000u) ? (T)-1 : (T)1;
+    const T* Jr = J + (size_t)((info >> 12) & 0xFFFu) * ncols;
+    const T* Cr = C + j * ncols;
+#pragma unroll
+    for (int u = 0; u < kRowsCols; u++) {
+      size_t col = c0 + (size_t)u * kRowsThreads;
+      if (ok[u]) acc[u] += (v + sg * Jr[col]) * Cr[col];
+    }
+  }
+  b = d_off[row];
+  e = d_off[row + 1];
+  for (int64_t k = b; k < e; k++) {
+    size_t j = (size_t)__ldg(&d_idx[k]);
+    T v = (T)__ldg(&d_val[k]);
+    const T* Cr = C + j * ncols;
+#pragma unroll
+    for (int u = 0; u < kRowsCols; u++) {
+      size_t col = c0 + (size_t)u * kRowsThreads;
+      if (ok[u]) acc[u] += v * Cr[col];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kRowsCols; u++) {
+    size_t col = c0 + (size_t)u * kRowsThreads;
+    if (ok[u]) S[row * ncols + col] = acc[u];
+  }
+}
+
 
 // Row stride (elements) of the integral block in shared memory: G values per
 // beta pair index rs, padded by 16 bytes so that the 16-byte vector loads of a
@@ -169,11 +225,23 @@ template <typename T>
 void sigma_launch(sbdgpu_ctx* c, const T* C, T* S, T* ct, T* st, const T* ja, const T* jb, const T* vf,
                   bool events) {
   cudaStream_t s = c->stream;
+  const SpinTables& ta = c->tab[0];
+  const SpinTables& tb = c->tab[1];
   if (events) SBD_CUDA(cudaEventRecord(c->ev[0], s));
-  same_spin_blocked<T, true>(c->blocks[0], C, S, c->na, c->nb, c->hii, jb, s);
+  {
+    dim3 g((unsigned)c->na, (unsigned)((c->nb + kRowsThreads * kRowsCols - 1) / (kRowsThreads * kRowsCols)));
+    rows_kernel<T, true><<<g, kRowsThreads, 0, s>>>(C, S, c->nb, c->hii, ta.s_off, ta.s_idx, ta.s_info, ta.s_val,
+                                                    ta.d_off, ta.d_idx, ta.d_val, jb);
+    SBD_CUDA(cudaGetLastError());
+  }
   if (events) SBD_CUDA(cudaEventRecord(c->ev[1], s));
   transpose(C, ct, c->na, c->nb, s);
-  same_spin_blocked<T, false>(c->blocks[1], ct, st, c->nb, c->na, nullptr, ja, s);
+  {
+    dim3 g((unsigned)c->nb, (unsigned)((c->na + kRowsThreads * kRowsCols - 1) / (kRowsThreads * kRowsCols)));
+    rows_kernel<T, false><<<g, kRowsThreads, 0, s>>>(ct, st, c->na, nullptr, tb.s_off, tb.s_idx, tb.s_info,
+                                                     tb.s_val, tb.d_off, tb.d_idx, tb.d_val, ja);
+    SBD_CUDA(cudaGetLastError());
+  }
   transpose_add(st, S, c->nb, c->na, s);
   if (events) SBD_CUDA(cudaEventRecord(c->ev[2], s));
   int dev_smem = 0;

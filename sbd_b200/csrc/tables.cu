@@ -195,8 +195,6 @@ void build_tables(sbdgpu_ctx* c) {
   if (c->tables_ready) return;
   build_one(c, c->tab[0], c->astr, c->na);
   build_one(c, c->tab[1], c->bstr, c->nb);
-  build_row_blocks(c, 0, kRowBlock);
-  build_row_blocks(c, 1, kRowBlock);
   c->tables_ready = true;
 }
 
