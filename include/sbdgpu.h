@@ -45,6 +45,10 @@ typedef struct sbdgpu_ctx sbdgpu_ctx;
 #define SBDGPU_FP64 0  /* plain path: every product and sum in FP64 */
 #define SBDGPU_MIXED 1 /* FP32 vectors and FP32 sigma; FP64 dot products, Ritz
                           step, residual norms and a final FP64 refinement sigma */
+#define SBDGPU_MIXED_TC 2 /* as SBDGPU_MIXED, with the alpha-beta term of sigma on the
+                             tensor cores (BF16 operands, FP32 accumulation); the
+                             Davidson switches to FP32 sigma once the residual norm
+                             is below 1e-2, then refines in FP64 */
 
 /* Davidson options: the reference SBD fields that steer the solver
  * (chemistry/tpb/sbdiag.h:12-30). */
@@ -53,7 +57,7 @@ typedef struct sbdgpu_opts {
   int max_nb;       /* SBD::max_nb (--block), Krylov block <= 32 */
   double eps;       /* SBD::eps (--tolerance), residual-norm target */
   double max_time;  /* SBD::max_time, wall-time budget in seconds */
-  int precision;    /* SBDGPU_FP64 or SBDGPU_MIXED */
+  int precision;    /* SBDGPU_FP64, SBDGPU_MIXED or SBDGPU_MIXED_TC */
   int verbose;      /* 1: print the reference's "Davidson iteration" lines */
 } sbdgpu_opts;
 

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libsbdgpu.so")
 
 FP64 = 0
 MIXED = 1
+MIXED_TC = 2
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _dp = ctypes.POINTER(ctypes.c_double)

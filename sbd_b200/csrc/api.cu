@@ -113,7 +113,7 @@ int guarded(sbdgpu_ctx* c, F&& f) {
 using sbdgpu::ensure_io;
 
 void check_precision(int precision) {
-  if (precision != SBDGPU_FP64 && precision != SBDGPU_MIXED)
+  if (precision != SBDGPU_FP64 && precision != SBDGPU_MIXED && precision != SBDGPU_MIXED_TC)
     throw Error{SBDGPU_ERR_ARG, "unsupported precision " + std::to_string(precision)};
 }
 
@@ -123,16 +123,19 @@ void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS, int preci
   sbdgpu::build_tables(c);
   sbdgpu::compute_hii(c);
   sbdgpu::ensure_scratch(c);
-  if (precision == SBDGPU_MIXED) sbdgpu::ensure_fp32(c);
+  if (precision != SBDGPU_FP64) sbdgpu::ensure_fp32(c);
   SBD_CUDA(cudaEventRecord(c->ev[4], c->stream));
   SBD_CUDA(cudaMemcpyAsync(c->io_a, dC, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, c->stream));
   sbdgpu::apply_phase(c, c->io_a);
-  if (precision == SBDGPU_MIXED) {
+  if (precision != SBDGPU_FP64) {
     if (!c->io32) c->io32 = (float*)sbdgpu::dev_alloc(sizeof(float) * 2 * c->N);
     float* c32 = c->io32;
     float* s32 = c->io32 + c->N;
     sbdgpu::convert(c->io_a, c32, c->N, c->stream);
-    sbdgpu::sigma_fp32(c, c32, s32);
+    if (precision == SBDGPU_MIXED_TC)
+      sbdgpu::sigma_fp32_tc(c, c32, s32);
+    else
+      sbdgpu::sigma_fp32(c, c32, s32);
     sbdgpu::convert(s32, dS, c->N, c->stream);
   } else {
     sbdgpu::sigma_fp64(c, c->io_a, dS);
@@ -143,6 +146,8 @@ void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS, int preci
   for (int k = 0; k < 3; k++) SBD_CUDA(cudaEventElapsedTime(&c->last_ms[k], c->ev[k], c->ev[k + 1]));
   SBD_CUDA(cudaEventElapsedTime(&c->last_ms[3], c->ev[4], c->ev[5]));
   c->last_ms[4] = 0.0f;
+  if (precision == SBDGPU_MIXED_TC && sbdgpu::tc_error(c))
+    throw Error{SBDGPU_ERR_CUDA, "tensor-core alpha-beta kernel: completion wait timed out"};
 }
 
 // Mixed-precision Davidson: FP32 basis and FP32 sigma; FP64 dot products,
@@ -152,6 +157,10 @@ void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS, int preci
 // chemistry/tpb/sbdiag.h:239-262).  Vectors in the alpha-string-major convention.
 void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, double* energy, double* trace_e,
                     double* trace_tol, int max_trace, int* n_steps) {
+  // SBDGPU_MIXED_TC: tensor-core sigma while the residual norm is above this,
+  // then a restart from the current Ritz vector with FP32 sigma
+  const double tc_switch = 1.0e-2;
+  bool use_tc = o->precision == SBDGPU_MIXED_TC && sbdgpu::tc_ab_supported(c);
   int nb = o->max_nb;
   size_t n = c->N;
   cudaStream_t st = c->stream;
@@ -183,7 +192,10 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
     sbdgpu::convert(W, C[0], n, st);
     for (int ib = 0; ib < nb; ib++) {
       auto t0 = std::chrono::steady_clock::now();
-      sbdgpu::sigma_fp32(c, C[ib], HC[ib]);
+      if (use_tc)
+        sbdgpu::sigma_fp32_tc(c, C[ib], HC[ib]);
+      else
+        sbdgpu::sigma_fp32(c, C[ib], HC[ib]);
       for (int jb = 0; jb <= ib; jb++) {
         H[jb + nb * ib] = sbdgpu::dot_f(c, C[jb], nullptr, HC[ib], n);
         H[ib + nb * jb] = H[jb + nb * ib];
@@ -208,6 +220,11 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
         cont = false;
         break;
       }
+      if (use_tc && tol < tc_switch) {
+        if (sbdgpu::tc_error(c)) throw Error{SBDGPU_ERR_CUDA, "tensor-core alpha-beta kernel: completion wait timed out"};
+        use_tc = false;  // restart from W with the FP32 sigma
+        break;
+      }
       if (ib < nb - 1) {
         sbdgpu::precondition(R, c->hii, E[0], eps_reg, X, n, st);
         for (int kb = 0; kb < ib + 1; kb++) {
@@ -230,6 +247,8 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
       }
     }
   }
+  if (o->precision == SBDGPU_MIXED_TC && sbdgpu::tc_error(c))
+    throw Error{SBDGPU_ERR_CUDA, "tensor-core alpha-beta kernel: completion wait timed out"};
   sbdgpu::sigma_fp64(c, W, R);  // FP64 refinement sigma
   *energy = sbdgpu::dot(c, W, R, n);
   *n_steps = steps;
@@ -399,7 +418,7 @@ int sbdgpu_davidson(sbdgpu_ctx* c, const sbdgpu_opts* o, double* Wh, double* ene
     R = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
     SBD_CUDA(cudaMemcpyAsync(W, Wh, sizeof(double) * n, cudaMemcpyHostToDevice, st));
     sbdgpu::apply_phase(c, W);
-    if (o->precision == SBDGPU_MIXED) {
+    if (o->precision != SBDGPU_FP64) {
       double e = 0.0;
       int steps = 0;
       davidson_mixed(c, o, W, R, &e, trace_e, trace_tol, max_trace, &steps);
@@ -522,7 +541,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);
-  cudaFree(c->hii); cudaFree(c->io32); cudaFree(c->ja32); cudaFree(c->jb32); cudaFree(c->vf32);
+  cudaFree(c->hii); cudaFree(c->tc_bk_off); cudaFree(c->tc_bk_ent); cudaFree(c->tc_err); cudaFree(c->io32); cudaFree(c->ja32); cudaFree(c->jb32); cudaFree(c->vf32);
   cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);
   for (int k = 0; k < 8; k++)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);

@@ -81,6 +81,9 @@ struct sbdgpu_ctx {
   float* ja32 = nullptr; // FP32 copies for the mixed path
   float* jb32 = nullptr;
   float* vf32 = nullptr;
+  int64_t* tc_bk_off = nullptr;  // alpha singles bucketed for the tensor-core alpha-beta kernel
+  uint32_t* tc_bk_ent = nullptr;
+  int* tc_err = nullptr;
   sbdgpu::SpinTables tab[2];
   bool tables_ready = false;
   bool hii_ready = false;
@@ -130,10 +133,17 @@ void rdm(sbdgpu_ctx* c, const double* dW, double* one, double* two);
 void occupation(sbdgpu_ctx* c, const double* dW, double* dens);
 void alpha_weights(sbdgpu_ctx* c, const double* dW, double* D);
 
+// tc_ab.cu
+bool tc_ab_supported(const sbdgpu_ctx* c);
+void build_tc_buckets(sbdgpu_ctx* c);
+void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out);
+int tc_error(sbdgpu_ctx* c);
+
 // sigma.cu
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);
 void sigma_fp64_prepared(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st);
 void sigma_fp32(sbdgpu_ctx* c, const float* C, float* S);
+void sigma_fp32_tc(sbdgpu_ctx* c, const float* C, float* S);
 
 // api.cu
 void ensure_scratch(sbdgpu_ctx* c);

@@ -288,4 +288,40 @@ void sigma_fp32(sbdgpu_ctx* c, const float* C, float* S) {
                       c->vf32, true);
 }
 
+// FP32 sigma with the alpha-beta term on the tensor cores (BF16 operands,
+// FP32 accumulation); the same-spin terms as in sigma_fp32.
+void sigma_fp32_tc(sbdgpu_ctx* c, const float* C, float* S) {
+  build_tables(c);
+  compute_hii(c);
+  ensure_scratch(c);
+  ensure_fp32(c);
+  build_tc_buckets(c);
+  if (!tc_ab_supported(c)) throw Error{SBDGPU_ERR_LIMIT, "tensor-core alpha-beta kernel: basis or norb too large"};
+  const SpinTables& ta = c->tab[0];
+  const SpinTables& tb = c->tab[1];
+  cudaStream_t s = c->stream;
+  float* ct = reinterpret_cast<float*>(c->ct);
+  float* st = reinterpret_cast<float*>(c->st);
+  SBD_CUDA(cudaEventRecord(c->ev[0], s));
+  {
+    dim3 g((unsigned)c->na, (unsigned)((c->nb + kRowsThreads * kRowsCols - 1) / (kRowsThreads * kRowsCols)));
+    rows_kernel<float, true><<<g, kRowsThreads, 0, s>>>(C, S, c->nb, c->hii, ta.s_off, ta.s_idx, ta.s_info,
+                                                        ta.s_val, ta.d_off, ta.d_idx, ta.d_val, c->jb32);
+    SBD_CUDA(cudaGetLastError());
+  }
+  SBD_CUDA(cudaEventRecord(c->ev[1], s));
+  transpose(C, ct, c->na, c->nb, s);
+  {
+    dim3 g((unsigned)c->nb, (unsigned)((c->na + kRowsThreads * kRowsCols - 1) / (kRowsThreads * kRowsCols)));
+    rows_kernel<float, false><<<g, kRowsThreads, 0, s>>>(ct, st, c->na, nullptr, tb.s_off, tb.s_idx, tb.s_info,
+                                                         tb.s_val, tb.d_off, tb.d_idx, tb.d_val, c->ja32);
+    SBD_CUDA(cudaGetLastError());
+  }
+  transpose_add(st, S, c->nb, c->na, s);
+  SBD_CUDA(cudaEventRecord(c->ev[2], s));
+  tc_alpha_beta(c, ct, st);
+  transpose_add(st, S, c->nb, c->na, s);
+  SBD_CUDA(cudaEventRecord(c->ev[3], s));
+}
+
 }  // namespace sbdgpu

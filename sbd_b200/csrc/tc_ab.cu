@@ -1,0 +1,315 @@
+// Alpha-beta sigma term on the 5th-generation tensor cores (tcgen05, BF16 in,
+// FP32 accumulation in tensor memory).
+//
+//   sigma[ia,ib] += sum_{(ja,pq,sa) in S_a(ia)} sa * G_ib[pq][ja],
+//   G_ib[pq][ja]  = sum_{(jb,rs,sb) in S_b(ib)} (pq|rs) * sb * C[ja,jb]
+//
+// For one beta string ib the second line is a dense GEMM: M = folded alpha
+// pair index pq (P = L(L+1)/2 rows, tiles of 128), N = source alpha string ja
+// (tiles of 64), K = the beta singles of ib (chunks of 80).  One CTA owns one
+// ib at a time (persistent over ib), keeps the A operand (pq|rs_t) for the
+// current K chunk in shared memory, streams B = sb_t C[ja, jb_t] tiles from
+// the transposed vector, and issues tcgen05.mma from one thread into TMEM
+// (one 128 x 64 FP32 accumulator per M tile).  The epilogue reads TMEM
+// (tcgen05.ld), stages one M tile in shared memory and adds the entries that
+// are real alpha singles into the CTA's FP32 sigma column with shared-memory
+// atomics; the column is written once per ib into a [nb][na] buffer.
+//
+// Operands use the canonical K-major layout without swizzle: 8-row x 16-byte
+// core matrices, LBO = 128 B between core matrices along K, SBO = 10 x 128 B
+// between 8-row groups.  Every wait on the MMA completion barrier is bounded;
+// on timeout the kernel records an error, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace sbdgpu {
+
+namespace {
+
+constexpr int kTcThreads = 128;  // 4 warps: one TMEM lane quarter each
+constexpr int kTcN = 64;         // alpha strings (ja) per tile
+constexpr int kTcK = 80;         // beta singles per K chunk (5 MMA steps of 16)
+constexpr int kTcKSteps = kTcK / 16;
+constexpr int kTcChunks = kTcK / 8;             // 16-byte core-matrix columns along K
+constexpr uint32_t kLBO = 128;                  // bytes between K-adjacent core matrices
+constexpr uint32_t kSBO = kTcChunks * 128;      // bytes between 8-row groups
+constexpr int kTcMaxMTiles = 8;                 // 8 x 64 = 512 TMEM columns
+constexpr int kGStride = kTcN + 1;              // padded epilogue staging row
+constexpr long long kSpinLimit = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint32_t kmajor_offset(int row, int k) {
+  return (uint32_t)(row >> 3) * kSBO + (uint32_t)(k >> 3) * kLBO + (uint32_t)(row & 7) * 16u + (uint32_t)(k & 7) * 2u;
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t start) {
+  return (uint64_t)((start >> 4) & 0x3FFFu) | ((uint64_t)((kLBO >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((kSBO >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16, BF16 x BF16 -> F32, both K-major, M = 128, N = 64
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long long i = 0; i < kSpinLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+struct TcArgs {
+  const float* ct;       // C^T [nb][na], alpha-string-major sign convention
+  float* out;            // [nb][na] alpha-beta part of sigma, transposed
+  const float* vf;       // (pq|rs) folded, [P][P]
+  const int64_t* b_off;  // beta singles CSR by bra
+  const int32_t* b_idx;
+  const uint32_t* b_info;
+  const int64_t* bk_off;   // alpha-pair buckets by (ja tile, M tile)
+  const uint32_t* bk_ent;  // ja_local | pq_local<<6 | neg<<13 | ia<<14
+  int* err;
+  int na, nb, P, mtiles;
+};
+
+__global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* A = smem_raw;                                        // mtiles x 128 x kTcK bf16
+  unsigned char* B = A + (size_t)a.mtiles * 128 * kTcK * 2;           // kTcN x kTcK bf16
+  float* G = reinterpret_cast<float*>(B + (size_t)kTcN * kTcK * 2);   // 128 x kGStride
+  float* sig = G + 128 * kGStride;                                    // na
+  __shared__ int s_jb[kTcK];
+  __shared__ int s_rs[kTcK];
+  __shared__ float s_sb[kTcK];
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) uint64_t s_mbar;
+  __shared__ int s_fail;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t mbar = smem_addr(&s_mbar);
+  // TMEM columns: a power of two >= 64 per M tile, so small problems leave
+  // room for other CTAs on the SM
+  uint32_t ncols = 32;
+  while (ncols < (uint32_t)(a.mtiles * kTcN)) ncols <<= 1;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  uint32_t phase = 0;
+  const int ntiles = (a.na + kTcN - 1) / kTcN;
+  const int Mrows = a.mtiles * 128;
+
+  for (int ib = blockIdx.x; ib < a.nb && !s_fail; ib += gridDim.x) {
+    for (int i = tid; i < a.na; i += kTcThreads) sig[i] = 0.f;
+    const int64_t t0 = a.b_off[ib], t1 = a.b_off[ib + 1];
+    for (int64_t kc = t0; kc < t1 && !s_fail; kc += kTcK) {
+      __syncthreads();
+      for (int t = tid; t < kTcK; t += kTcThreads) {
+        int64_t k = kc + t;
+        if (k < t1) {
+          uint32_t info = a.b_info[k];
+          s_jb[t] = a.b_idx[k];
+          s_rs[t] = (info >> 12) & 0xFFFu;
+          s_sb[t] = (info & 0x80000000u) ? -1.f : 1.f;
+        } else {
+          s_jb[t] = -1;
+          s_rs[t] = -1;
+          s_sb[t] = 0.f;
+        }
+      }
+      __syncthreads();
+      // A[m][t] = (pq_m | rs_t); (pq|rs) is symmetric, so row rs_t of Vf is read
+      for (int idx = tid; idx < Mrows * kTcK; idx += kTcThreads) {
+        int t = idx / Mrows, m = idx - t * Mrows;
+        int rs = s_rs[t];
+        float v = (rs >= 0 && m < a.P) ? a.vf[(size_t)rs * a.P + m] : 0.f;
+        *reinterpret_cast<__nv_bfloat16*>(A + kmajor_offset(m, t)) = __float2bfloat16_rn(v);
+      }
+      for (int tile = 0; tile < ntiles && !s_fail; tile++) {
+        const int ja0 = tile * kTcN;
+        // B[n][t] = sb_t * C[ja0+n, jb_t]
+        for (int idx = tid; idx < kTcN * kTcK; idx += kTcThreads) {
+          int t = idx / kTcN, n = idx - t * kTcN;
+          int jb = s_jb[t], ja = ja0 + n;
+          float v = (jb >= 0 && ja < a.na) ? s_sb[t] * a.ct[(size_t)jb * a.na + ja] : 0.f;
+          *reinterpret_cast<__nv_bfloat16*>(B + kmajor_offset(n, t)) = __float2bfloat16_rn(v);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_addr(A), b0 = smem_addr(B);
+          for (int mt = 0; mt < a.mtiles; mt++)
+#pragma unroll
+            for (int ks = 0; ks < kTcKSteps; ks++)
+              mma_bf16(tmem + (uint32_t)(mt * kTcN), smem_desc(a0 + (uint32_t)mt * 16u * kSBO + ks * 2 * kLBO),
+                       smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
+          mma_commit(mbar);
+        }
+        if (!mbar_wait(mbar, phase)) {
+          if (tid == 0) atomicExch(a.err, 1);
+          s_fail = 1;
+        }
+        phase ^= 1u;
+        __syncthreads();
+        if (s_fail) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        for (int mt = 0; mt < a.mtiles; mt++) {
+          // TMEM lanes 32w..32w+31 hold rows pq = 128 mt + 32 w + lane
+          float v[16];
+#pragma unroll
+          for (int c4 = 0; c4 < kTcN / 16; c4++) {
+            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(mt * kTcN + 16 * c4), v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int i = 0; i < 16; i++) G[(32 * warp + lane) * kGStride + 16 * c4 + i] = v[i];
+          }
+          __syncthreads();
+          const int64_t e0 = a.bk_off[(size_t)tile * a.mtiles + mt], e1 = a.bk_off[(size_t)tile * a.mtiles + mt + 1];
+          for (int64_t e = e0 + tid; e < e1; e += kTcThreads) {
+            uint32_t en = a.bk_ent[e];
+            int jl = en & 63u, pl = (en >> 6) & 127u, ia = (int)(en >> 14);
+            float g = G[pl * kGStride + jl];
+            atomicAdd(&sig[ia], (en & (1u << 13)) ? -g : g);
+          }
+          __syncthreads();
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < a.na; i += kTcThreads) a.out[(size_t)ib * a.na + i] = sig[i];
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+}  // namespace
+
+bool tc_ab_supported(const sbdgpu_ctx* c) {
+  int mtiles = (c->P + 127) / 128;
+  size_t smem = (size_t)mtiles * 128 * kTcK * 2 + (size_t)kTcN * kTcK * 2 + 128 * kGStride * 4 + c->na * 4;
+  return mtiles <= kTcMaxMTiles && c->na <= (1 << 18) && smem <= 220 * 1024;
+}
+
+// Alpha singles bucketed by (tile of 64 source strings ja, M tile of 128 pq).
+void build_tc_buckets(sbdgpu_ctx* c) {
+  if (c->tc_bk_ent) return;
+  const SpinTables& ta = c->tab[0];
+  int mtiles = (c->P + 127) / 128;
+  size_t na = c->na;
+  std::vector<int32_t> idx(ta.ns);
+  std::vector<uint32_t> info(ta.ns);
+  if (ta.ns) {
+    SBD_CUDA(cudaMemcpy(idx.data(), ta.s_idx, sizeof(int32_t) * ta.ns, cudaMemcpyDeviceToHost));
+    SBD_CUDA(cudaMemcpy(info.data(), ta.s_info, sizeof(uint32_t) * ta.ns, cudaMemcpyDeviceToHost));
+  }
+  size_t ntiles = (na + kTcN - 1) / kTcN;
+  std::vector<std::vector<uint32_t>> bucket(ntiles * mtiles);
+  for (size_t ja = 0; ja < na; ja++) {
+    for (int64_t k = ta.h_s_off[ja]; k < ta.h_s_off[ja + 1]; k++) {
+      // row ja, ket ia: pair index and sign are those of the pair (ia <- ja)
+      uint32_t pq = (info[k] >> 12) & 0xFFFu;
+      uint32_t neg = (info[k] >> 31) & 1u;
+      uint32_t ia = (uint32_t)idx[k];
+      size_t tile = ja / kTcN;
+      uint32_t e = (uint32_t)(ja % kTcN) | ((pq % 128u) << 6) | (neg << 13) | (ia << 14);
+      bucket[tile * mtiles + pq / 128].push_back(e);
+    }
+  }
+  std::vector<int64_t> off(bucket.size() + 1, 0);
+  for (size_t i = 0; i < bucket.size(); i++) off[i + 1] = off[i] + (int64_t)bucket[i].size();
+  std::vector<uint32_t> ent((size_t)off.back());
+  for (size_t i = 0; i < bucket.size(); i++) std::copy(bucket[i].begin(), bucket[i].end(), ent.begin() + off[i]);
+  c->tc_bk_off = (int64_t*)dev_alloc(sizeof(int64_t) * off.size());
+  c->tc_bk_ent = (uint32_t*)dev_alloc(sizeof(uint32_t) * std::max<size_t>(ent.size(), 1));
+  SBD_CUDA(cudaMemcpy(c->tc_bk_off, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice));
+  if (!ent.empty())
+    SBD_CUDA(cudaMemcpy(c->tc_bk_ent, ent.data(), sizeof(uint32_t) * ent.size(), cudaMemcpyHostToDevice));
+  if (!c->tc_err) {
+    c->tc_err = (int*)dev_alloc(sizeof(int));
+    SBD_CUDA(cudaMemset(c->tc_err, 0, sizeof(int)));
+  }
+}
+
+// out[ib][ia] = alpha-beta part of sigma (FP32, transposed) from ct = C^T.
+void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
+  const SpinTables& tb = c->tab[1];
+  TcArgs a;
+  a.ct = ct;
+  a.out = out;
+  a.vf = c->vf32;
+  a.b_off = tb.s_off;
+  a.b_idx = tb.s_idx;
+  a.b_info = tb.s_info;
+  a.bk_off = c->tc_bk_off;
+  a.bk_ent = c->tc_bk_ent;
+  a.err = c->tc_err;
+  a.na = (int)c->na;
+  a.nb = (int)c->nb;
+  a.P = c->P;
+  a.mtiles = (c->P + 127) / 128;
+  size_t smem = (size_t)a.mtiles * 128 * kTcK * 2 + (size_t)kTcN * kTcK * 2 + 128 * kGStride * 4 + c->na * 4;
+  SBD_CUDA(cudaFuncSetAttribute(tc_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int sms = 148;
+  SBD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  int grid = (int)std::min<size_t>((size_t)sms, c->nb);
+  tc_ab_kernel<<<grid, kTcThreads, smem, c->stream>>>(a);
+  SBD_CUDA(cudaGetLastError());
+}
+
+int tc_error(sbdgpu_ctx* c) {
+  if (!c->tc_err) return 0;
+  int h = 0;
+  SBD_CUDA(cudaMemcpyAsync(&h, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+  return h;
+}
+
+}  // namespace sbdgpu
