@@ -260,7 +260,11 @@ def time_to_e0(ctx, args):
     t = time.perf_counter()
     e_mix, _, tm, ttm = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED)
     t_mixed = time.perf_counter() - t
-    return {"e_fp64": e_ref, "e_mixed": e_mix, "abs_err_mixed": abs(e_mix - e_ref),
+    t = time.perf_counter()
+    e_tc, _, ttc, tttc = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED_TC)
+    t_tc = time.perf_counter() - t
+    return {"e_mixed_tc": e_tc, "abs_err_mixed_tc": abs(e_tc - e_ref), "mixed_tc_steps": len(ttc),
+            "mixed_tc_s": t_tc, "speedup_tc": t_plain / t_tc,"e_fp64": e_ref, "e_mixed": e_mix, "abs_err_mixed": abs(e_mix - e_ref),
             "plain_steps_total": len(te), "plain_steps_to_1e-6": k, "plain_s_to_1e-6": t_plain,
             "plain_final_residual": float(tt[-1]), "mixed_steps": len(tm), "mixed_s": t_mixed,
             "mixed_final_residual": float(ttm[-1]), "speedup": t_plain / t_mixed,
@@ -311,6 +315,11 @@ def run_gpu(args):
         ctx.sigma_device(C.data_ptr(), S.data_ptr(), precision=sbd_b200.MIXED)
         if i >= args.warmup:
             mixed_ms.append(ctx.last_sigma_ms())
+    tc_ms = []
+    for i in range(args.warmup + args.steps):
+        ctx.sigma_device(C.data_ptr(), S.data_ptr(), precision=sbd_b200.MIXED_TC)
+        if i >= args.warmup:
+            tc_ms.append(ctx.last_sigma_ms())
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
@@ -374,6 +383,9 @@ def run_gpu(args):
         "mixed_fp32": {"sigma_per_s": 1000.0 * len(mixed_ms) / sum(m[3] for m in mixed_ms),
                        "phases_ms": [sum(m[k] for m in mixed_ms) / len(mixed_ms) for k in range(3)],
                        "note": "FP32 vectors and sigma incl. FP64<->FP32 conversion at the ABI"},
+        "mixed_tc": {"sigma_per_s": 1000.0 * len(tc_ms) / sum(m[3] for m in tc_ms),
+                     "phases_ms": [sum(m[k] for m in tc_ms) / len(tc_ms) for k in range(3)],
+                     "note": "FP32 vectors; alpha-beta term on tcgen05 tensor cores (BF16 operands, FP32 accumulation)"},
         "clocks": sampler.summary(),
     }
     if args.time_to_e0:
