@@ -159,8 +159,12 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
                     double* trace_tol, int max_trace, int* n_steps) {
   // SBDGPU_MIXED_TC: tensor-core sigma while the residual norm is above this,
   // then a restart from the current Ritz vector with FP32 sigma
+  // (or when the BF16 operator stops improving the residual: a whole restart
+  // cycle that gains less than 30 %, or 40 steps)
   const double tc_switch = 1.0e-2;
   bool use_tc = o->precision == SBDGPU_MIXED_TC && sbdgpu::tc_ab_supported(c);
+  double tol_cycle = 1e300;
+  int tc_steps = 0;
   int nb = o->max_nb;
   size_t n = c->N;
   cudaStream_t st = c->stream;
@@ -220,10 +224,19 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
         cont = false;
         break;
       }
-      if (use_tc && tol < tc_switch) {
-        if (sbdgpu::tc_error(c)) throw Error{SBDGPU_ERR_CUDA, "tensor-core alpha-beta kernel: completion wait timed out"};
-        use_tc = false;  // restart from W with the FP32 sigma
-        break;
+      if (use_tc) {
+        tc_steps++;
+        bool stalled = false;
+        if (ib == nb - 1) {
+          stalled = tol > 0.7 * tol_cycle;
+          tol_cycle = tol;
+        }
+        if (tol < tc_switch || stalled || tc_steps >= 40) {
+          if (sbdgpu::tc_error(c))
+            throw Error{SBDGPU_ERR_CUDA, "tensor-core alpha-beta kernel: completion wait timed out"};
+          use_tc = false;  // restart from W with the FP32 sigma
+          break;
+        }
       }
       if (ib < nb - 1) {
         sbdgpu::precondition(R, c->hii, E[0], eps_reg, X, n, st);
@@ -541,7 +554,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);
-  cudaFree(c->hii); cudaFree(c->tc_bk_off); cudaFree(c->tc_bk_ent); cudaFree(c->tc_err); cudaFree(c->io32); cudaFree(c->ja32); cudaFree(c->jb32); cudaFree(c->vf32);
+  cudaFree(c->hii); cudaFree(c->tc_bk_off); cudaFree(c->tc_bk_ent); cudaFree(c->tc_err); cudaFree(c->ct16); cudaFree(c->io32); cudaFree(c->ja32); cudaFree(c->jb32); cudaFree(c->vf32);
   cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);
   for (int k = 0; k < 8; k++)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);

@@ -84,6 +84,7 @@ struct sbdgpu_ctx {
   int64_t* tc_bk_off = nullptr;  // alpha singles bucketed for the tensor-core alpha-beta kernel
   uint32_t* tc_bk_ent = nullptr;
   int* tc_err = nullptr;
+  void* ct16 = nullptr;  // BF16 copy of C^T, rows padded to 64 (tensor-core path)
   sbdgpu::SpinTables tab[2];
   bool tables_ready = false;
   bool hii_ready = false;

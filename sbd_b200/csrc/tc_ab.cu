@@ -30,7 +30,7 @@ namespace sbdgpu {
 
 namespace {
 
-constexpr int kTcThreads = 128;  // 4 warps: one TMEM lane quarter each
+constexpr int kTcThreads = 256;  // 8 warps: warp w reads TMEM lane quarter w % 4, column half w / 4
 constexpr int kTcN = 64;         // alpha strings (ja) per tile
 constexpr int kTcK = 80;         // beta singles per K chunk (5 MMA steps of 16)
 constexpr int kTcKSteps = kTcK / 16;
@@ -52,8 +52,21 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t start) {
          ((uint64_t)((kSBO >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// kind::f16, BF16 x BF16 -> F32, both K-major, M = 128, N = 64
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) | ((128u >> 4) << 24);
+// kind::f16, BF16 x BF16 -> F32, A K-major, B MN-major (bit 16), M = 128, N = 64
+constexpr uint32_t kIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(kTcN >> 3) << 17) | ((128u >> 4) << 24);
+
+// MN-major canonical layout (no swizzle) of B = [K = t][N = ja]: core matrix =
+// 8 K-rows x 16 bytes (8 consecutive ja); LBO between K groups, SBO between
+// 8-ja groups.  Offsets are 16-byte aligned per 8-ja chunk, so each chunk is
+// one cp.async from a row of the BF16 transposed vector.
+__device__ __forceinline__ uint32_t mnmajor_chunk_offset(int n8, int t) {
+  return (uint32_t)n8 * kSBO + (uint32_t)(t >> 3) * kLBO + (uint32_t)(t & 7) * 16u;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
 
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
   asm volatile(
@@ -93,7 +106,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 struct TcArgs {
-  const float* ct;       // C^T [nb][na], alpha-string-major sign convention
+  const __nv_bfloat16* ct16;  // C^T in BF16, [nb][na_pad] (zero padded), alpha-string-major convention
   float* out;            // [nb][na] alpha-beta part of sigma, transposed
   const float* vf;       // (pq|rs) folded, [P][P]
   const int64_t* b_off;  // beta singles CSR by bra
@@ -102,15 +115,16 @@ struct TcArgs {
   const int64_t* bk_off;   // alpha-pair buckets by (ja tile, M tile)
   const uint32_t* bk_ent;  // ja_local | pq_local<<6 | neg<<13 | ia<<14
   int* err;
-  int na, nb, P, mtiles;
+  int na, nb, P, mtiles, na_pad;
 };
 
 __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char* A = smem_raw;                                        // mtiles x 128 x kTcK bf16
-  unsigned char* B = A + (size_t)a.mtiles * 128 * kTcK * 2;           // kTcN x kTcK bf16
-  float* G = reinterpret_cast<float*>(B + (size_t)kTcN * kTcK * 2);   // 128 x kGStride
-  float* sig = G + 128 * kGStride;                                    // na
+  constexpr uint32_t kBBytes = (uint32_t)kTcN * kTcK * 2;
+  unsigned char* A = smem_raw;                                      // mtiles x 128 x kTcK bf16, K-major
+  unsigned char* Bb = A + (size_t)a.mtiles * 128 * kTcK * 2;        // 2 x (kTcK x kTcN bf16), MN-major
+  float* G = reinterpret_cast<float*>(Bb + 2 * (size_t)kBBytes);    // 128 x kGStride
+  float* sig = G + 128 * kGStride;                                  // na
   __shared__ int s_jb[kTcK];
   __shared__ int s_rs[kTcK];
   __shared__ float s_sb[kTcK];
@@ -119,6 +133,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   __shared__ int s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quarter = warp & 3, half = warp >> 2;
   const uint32_t mbar = smem_addr(&s_mbar);
   // TMEM columns: a power of two >= 64 per M tile, so small problems leave
   // room for other CTAs on the SM
@@ -141,6 +156,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   uint32_t phase = 0;
   const int ntiles = (a.na + kTcN - 1) / kTcN;
   const int Mrows = a.mtiles * 128;
+  const uint32_t b_base = smem_addr(Bb);
+
+  // B tile `tile` -> buffer `buf`: 8 chunks of 8 alpha strings per beta single t
+  auto load_b = [&](int tile, int buf) {
+    const int ja0 = tile * kTcN;
+    for (int idx = tid; idx < kTcK * (kTcN / 8); idx += kTcThreads) {
+      int t = idx >> 3, n8 = idx & 7;
+      int jb = s_jb[t];
+      const __nv_bfloat16* src = jb >= 0 ? a.ct16 + (size_t)jb * a.na_pad + ja0 + 8 * n8 : a.ct16;
+      cp_async16(b_base + (uint32_t)buf * kBBytes + mnmajor_chunk_offset(n8, t), src, jb >= 0 ? 16u : 0u);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
 
   for (int ib = blockIdx.x; ib < a.nb && !s_fail; ib += gridDim.x) {
     for (int i = tid; i < a.na; i += kTcThreads) sig[i] = 0.f;
@@ -161,28 +189,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
         }
       }
       __syncthreads();
-      // A[m][t] = (pq_m | rs_t); (pq|rs) is symmetric, so row rs_t of Vf is read
+      load_b(0, 0);
+      // A[m][t] = sb_t (pq_m | rs_t); (pq|rs) is symmetric, so row rs_t of Vf is read
       for (int idx = tid; idx < Mrows * kTcK; idx += kTcThreads) {
         int t = idx / Mrows, m = idx - t * Mrows;
         int rs = s_rs[t];
-        float v = (rs >= 0 && m < a.P) ? a.vf[(size_t)rs * a.P + m] : 0.f;
+        float v = (rs >= 0 && m < a.P) ? s_sb[t] * a.vf[(size_t)rs * a.P + m] : 0.f;
         *reinterpret_cast<__nv_bfloat16*>(A + kmajor_offset(m, t)) = __float2bfloat16_rn(v);
       }
       for (int tile = 0; tile < ntiles && !s_fail; tile++) {
-        const int ja0 = tile * kTcN;
-        // B[n][t] = sb_t * C[ja0+n, jb_t]
-        for (int idx = tid; idx < kTcN * kTcK; idx += kTcThreads) {
-          int t = idx / kTcN, n = idx - t * kTcN;
-          int jb = s_jb[t], ja = ja0 + n;
-          float v = (jb >= 0 && ja < a.na) ? s_sb[t] * a.ct[(size_t)jb * a.na + ja] : 0.f;
-          *reinterpret_cast<__nv_bfloat16*>(B + kmajor_offset(n, t)) = __float2bfloat16_rn(v);
-        }
+        const int buf = tile & 1;
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t a0 = smem_addr(A), b0 = smem_addr(B);
+          const uint32_t a0 = smem_addr(A), b0 = b_base + (uint32_t)buf * kBBytes;
           for (int mt = 0; mt < a.mtiles; mt++)
 #pragma unroll
             for (int ks = 0; ks < kTcKSteps; ks++)
@@ -190,6 +213,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
                        smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
           mma_commit(mbar);
         }
+        // the other buffer was read by the previous tile's MMAs, which completed
+        if (tile + 1 < ntiles) load_b(tile + 1, buf ^ 1);
         if (!mbar_wait(mbar, phase)) {
           if (tid == 0) atomicExch(a.err, 1);
           s_fail = 1;
@@ -199,14 +224,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
         if (s_fail) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         for (int mt = 0; mt < a.mtiles; mt++) {
-          // TMEM lanes 32w..32w+31 hold rows pq = 128 mt + 32 w + lane
+          // TMEM lanes 32q..32q+31 hold rows pq = 128 mt + 32 q + lane; columns split by half
           float v[16];
 #pragma unroll
-          for (int c4 = 0; c4 < kTcN / 16; c4++) {
-            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(mt * kTcN + 16 * c4), v);
+          for (int c = 0; c < 2; c++) {
+            const int col = 32 * half + 16 * c;
+            tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(mt * kTcN + col), v);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int i = 0; i < 16; i++) G[(32 * warp + lane) * kGStride + 16 * c4 + i] = v[i];
+            for (int i = 0; i < 16; i++) G[(32 * quarter + lane) * kGStride + col + i] = v[i];
           }
           __syncthreads();
           const int64_t e0 = a.bk_off[(size_t)tile * a.mtiles + mt], e1 = a.bk_off[(size_t)tile * a.mtiles + mt + 1];
@@ -220,22 +246,36 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       }
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     }
     __syncthreads();
     for (int i = tid; i < a.na; i += kTcThreads) a.out[(size_t)ib * a.na + i] = sig[i];
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
 
+__global__ void to_bf16_padded_kernel(const float* __restrict__ in, __nv_bfloat16* __restrict__ out, size_t rows,
+                                      size_t cols, size_t cols_pad) {
+  size_t n = rows * cols_pad;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    size_t r = i / cols_pad, cc = i - r * cols_pad;
+    out[i] = __float2bfloat16_rn(cc < cols ? in[r * cols + cc] : 0.f);
+  }
+}
+
+size_t tc_smem_bytes(int mtiles, size_t na) {
+  return (size_t)mtiles * 128 * kTcK * 2 + 2 * (size_t)kTcN * kTcK * 2 + 128 * kGStride * 4 + na * 4;
+}
+
 }  // namespace
 
 bool tc_ab_supported(const sbdgpu_ctx* c) {
   int mtiles = (c->P + 127) / 128;
-  size_t smem = (size_t)mtiles * 128 * kTcK * 2 + (size_t)kTcN * kTcK * 2 + 128 * kGStride * 4 + c->na * 4;
-  return mtiles <= kTcMaxMTiles && c->na <= (1 << 18) && smem <= 220 * 1024;
+  return mtiles <= kTcMaxMTiles && c->na <= (1 << 18) && tc_smem_bytes(mtiles, c->na) <= 225 * 1024;
 }
 
 // Alpha singles bucketed by (tile of 64 source strings ja, M tile of 128 pq).
@@ -281,8 +321,14 @@ void build_tc_buckets(sbdgpu_ctx* c) {
 // out[ib][ia] = alpha-beta part of sigma (FP32, transposed) from ct = C^T.
 void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
   const SpinTables& tb = c->tab[1];
+  size_t na_pad = (c->na + kTcN - 1) / kTcN * kTcN;
+  if (!c->ct16) c->ct16 = dev_alloc(sizeof(__nv_bfloat16) * na_pad * c->nb);
+  __nv_bfloat16* ct16 = static_cast<__nv_bfloat16*>(c->ct16);
+  to_bf16_padded_kernel<<<592, 256, 0, c->stream>>>(ct, ct16, c->nb, c->na, na_pad);
+  SBD_CUDA(cudaGetLastError());
   TcArgs a;
-  a.ct = ct;
+  a.ct16 = ct16;
+  a.na_pad = (int)na_pad;
   a.out = out;
   a.vf = c->vf32;
   a.b_off = tb.s_off;
@@ -295,7 +341,7 @@ void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
   a.nb = (int)c->nb;
   a.P = c->P;
   a.mtiles = (c->P + 127) / 128;
-  size_t smem = (size_t)a.mtiles * 128 * kTcK * 2 + (size_t)kTcN * kTcK * 2 + 128 * kGStride * 4 + c->na * 4;
+  size_t smem = tc_smem_bytes(a.mtiles, c->na);
   SBD_CUDA(cudaFuncSetAttribute(tc_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int sms = 148;
   SBD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
