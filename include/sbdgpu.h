@@ -59,6 +59,10 @@ typedef struct sbdgpu_opts {
   double max_time;  /* SBD::max_time, wall-time budget in seconds */
   int precision;    /* SBDGPU_FP64, SBDGPU_MIXED or SBDGPU_MIXED_TC */
   int verbose;      /* 1: print the reference's "Davidson iteration" lines */
+  int restart_keep; /* mixed precisions only: Ritz vectors kept at a restart; 0 or 1 =
+                       the reference's collapse to the lowest Ritz vector
+                       (davidson.h:911-915), k > 1 = thick restart with the k lowest,
+                       whose sigma vectors are carried over instead of recomputed */
 } sbdgpu_opts;
 
 /* Create a context on CUDA device `device` for one alpha x beta product basis

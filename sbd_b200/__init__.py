@@ -36,7 +36,8 @@ class SbdGpuError(RuntimeError):
 
 class Opts(ctypes.Structure):
     _fields_ = [("max_it", ctypes.c_int), ("max_nb", ctypes.c_int), ("eps", ctypes.c_double),
-                ("max_time", ctypes.c_double), ("precision", ctypes.c_int), ("verbose", ctypes.c_int)]
+                ("max_time", ctypes.c_double), ("precision", ctypes.c_int), ("verbose", ctypes.c_int),
+                ("restart_keep", ctypes.c_int)]
 
 
 _lib = None
@@ -148,9 +149,9 @@ class Context:
         return [float(x) for x in a]
 
     def davidson(self, W0: np.ndarray, max_it: int, max_nb: int, eps: float, max_time: float = 86400.0,
-                 precision: int = FP64, verbose: int = 0, max_trace: int = 100000):
+                 precision: int = FP64, verbose: int = 0, max_trace: int = 100000, restart_keep: int = 0):
         W = np.ascontiguousarray(W0, dtype=np.float64).ravel().copy()
-        o = Opts(max_it, max_nb, eps, max_time, precision, verbose)
+        o = Opts(max_it, max_nb, eps, max_time, precision, verbose, restart_keep)
         e = ctypes.c_double(0.0)
         te = np.zeros(max_trace)
         tt = np.zeros(max_trace)

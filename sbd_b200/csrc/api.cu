@@ -192,9 +192,37 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
   auto t_start = std::chrono::steady_clock::now();
   int steps = 0;
   bool cont = true;
+  const int keep = std::min(std::max(o->restart_keep, 1), nb - 1);
+  std::vector<float*> T(keep, nullptr), TH(keep, nullptr);
+  struct FreeT {
+    std::vector<float*>* a;
+    std::vector<float*>* b;
+    ~FreeT() {
+      for (auto p : *a) cudaFree(p);
+      for (auto p : *b) cudaFree(p);
+    }
+  } guard_t{&T, &TH};
+  if (keep > 1)
+    for (int j = 0; j < keep; j++) {
+      T[j] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
+      TH[j] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
+    }
+  int kept = 0;  // basis vectors (with their sigma) carried into the next cycle
+  auto add_correction = [&](int into, double e0) {
+    sbdgpu::precondition(R, c->hii, e0, eps_reg, X, n, st);
+    for (int kb = 0; kb < into; kb++) {
+      double olap = sbdgpu::dot_f(c, C[kb], X, C[kb], n);  // <X|C_kb> with X in FP64
+      sbdgpu::axpy_df(X, C[kb], -olap, n, st);
+    }
+    double nc = std::sqrt(sbdgpu::dot(c, X, X, n));
+    sbdgpu::scale(X, 1.0 / nc, n, st);
+    sbdgpu::convert(X, C[into], n, st);
+  };
   for (int it = 0; it < o->max_it && cont; it++) {
-    sbdgpu::convert(W, C[0], n, st);
-    for (int ib = 0; ib < nb; ib++) {
+    int ib0 = kept;
+    if (kept == 0) sbdgpu::convert(W, C[0], n, st);
+    kept = 0;
+    for (int ib = ib0; ib < nb; ib++) {
       auto t0 = std::chrono::steady_clock::now();
       if (use_tc)
         sbdgpu::sigma_fp32_tc(c, C[ib], HC[ib]);
@@ -234,19 +262,31 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
         if (tol < tc_switch || stalled || tc_steps >= 40) {
           if (sbdgpu::tc_error(c))
             throw Error{SBDGPU_ERR_CUDA, "tensor-core alpha-beta kernel: completion wait timed out"};
-          use_tc = false;  // restart from W with the FP32 sigma
+          use_tc = false;  // restart from W alone, so every sigma comes from the FP32 operator
           break;
         }
       }
       if (ib < nb - 1) {
-        sbdgpu::precondition(R, c->hii, E[0], eps_reg, X, n, st);
-        for (int kb = 0; kb < ib + 1; kb++) {
-          double olap = sbdgpu::dot_f(c, C[kb], X, C[kb], n);  // <X|C_kb> with X in FP64
-          sbdgpu::axpy_df(X, C[kb], -olap, n, st);
+        add_correction(ib + 1, E[0]);
+      } else if (keep > 1) {
+        // thick restart: the keep lowest Ritz vectors and their sigma vectors
+        std::vector<double> col(nb);
+        for (int j = 0; j < keep; j++) {
+          for (int i = 0; i < nb; i++) col[i] = U[i + nb * j];
+          sbdgpu::lincomb_f(C.data(), col.data(), nb, T[j], n, c);
+          sbdgpu::lincomb_f(HC.data(), col.data(), nb, TH[j], n, c);
         }
-        double nc = std::sqrt(sbdgpu::dot(c, X, X, n));
-        sbdgpu::scale(X, 1.0 / nc, n, st);
-        sbdgpu::convert(X, C[ib + 1], n, st);
+        for (int j = 0; j < keep; j++) {
+          std::swap(C[j], T[j]);
+          std::swap(HC[j], TH[j]);
+        }
+        for (int j = 0; j < keep; j++)
+          for (int i = 0; i <= j; i++) {
+            H[i + nb * j] = sbdgpu::dot_f(c, C[i], nullptr, HC[j], n);
+            H[j + nb * i] = H[i + nb * j];
+          }
+        add_correction(keep, E[0]);
+        kept = keep;
       }
       SBD_CUDA(cudaStreamSynchronize(st));
       auto t1 = std::chrono::steady_clock::now();

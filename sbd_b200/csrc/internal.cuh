@@ -121,6 +121,7 @@ double dot(sbdgpu_ctx* c, const double* x, const double* y, size_t n);
 void scale(double* x, double a, size_t n, cudaStream_t s);
 double dot_f(sbdgpu_ctx* c, const float* x, const double* xd, const float* y, size_t n);
 void axpy_df(double* y, const float* x, double a, size_t n, cudaStream_t s);
+void lincomb_f(float* const* in, const double* U, int nk, float* out, size_t n, sbdgpu_ctx* c);
 void convert(const double* in, float* out, size_t n, cudaStream_t s);
 void convert(const float* in, double* out, size_t n, cudaStream_t s);
 void ritz_update_f(float* const* C, float* const* HC, const double* U, int nk, double e0, double* W, double* R,

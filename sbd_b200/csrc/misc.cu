@@ -193,6 +193,16 @@ __global__ void ritz_kernel_f(PtrPackF c, PtrPackF hc, const double* __restrict_
   }
 }
 
+// out = sum_k u_k in_k (FP32 vectors, FP64 accumulation)
+__global__ void lincomb_kernel_f(PtrPackF in, const double* __restrict__ u, int nk, float* __restrict__ out,
+                                 size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int k = 0; k < nk; k++) acc += (double)in.p[k][i] * u[k];
+    out[i] = (float)acc;
+  }
+}
+
 struct PtrPack {
   const double* p[32];
   double u[32];
@@ -531,6 +541,17 @@ void ritz_update_f(float* const* C, float* const* HC, const double* U, int nk, d
   double* du = c->red + 600;  // 32 spare doubles after the 593 reduction slots
   SBD_CUDA(cudaMemcpyAsync(du, U, sizeof(double) * nk, cudaMemcpyHostToDevice, c->stream));
   ritz_kernel_f<<<grid_for(n), 256, 0, c->stream>>>(pc, ph, du, nk, e0, W, R, n);
+  SBD_CUDA(cudaGetLastError());
+  SBD_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+void lincomb_f(float* const* in, const double* U, int nk, float* out, size_t n, sbdgpu_ctx* c) {
+  PtrPackF p{};
+  for (int k = 0; k < nk; k++) p.p[k] = in[k];
+  ensure_scratch(c);
+  double* du = c->red + 640;
+  SBD_CUDA(cudaMemcpyAsync(du, U, sizeof(double) * nk, cudaMemcpyHostToDevice, c->stream));
+  lincomb_kernel_f<<<grid_for(n), 256, 0, c->stream>>>(p, du, nk, out, n);
   SBD_CUDA(cudaGetLastError());
   SBD_CUDA(cudaStreamSynchronize(c->stream));
 }

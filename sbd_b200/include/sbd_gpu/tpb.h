@@ -451,7 +451,7 @@ inline void diag(const MPI_Comm& comm, const SBD& sbd_data, const FCIDump& fcidu
     std::cout << " method " << sbd_data.method
               << ": the GPU path builds H*C on the fly (method 0); results are the same" << std::endl;
   auto t_diag = std::chrono::high_resolution_clock::now();
-  sbdgpu_opts o{sbd_data.max_it, sbd_data.max_nb, sbd_data.eps, sbd_data.max_time, sbd_data.precision, 1};
+  sbdgpu_opts o{sbd_data.max_it, sbd_data.max_nb, sbd_data.eps, sbd_data.max_time, sbd_data.precision, 1, 0};
   double e = 0.0;
   int steps = 0;
   g.check(sbdgpu_davidson(g.c, &o, W.data(), &e, nullptr, nullptr, 0, &steps), "sbdgpu_davidson");

@@ -31,3 +31,18 @@ def test_mixed_davidson_energy(golden):
     assert abs(e - float(golden["energy"])) < 1e-6
     assert tt[-1] < 1e-4
     assert abs(abs(np.dot(W, golden["W"])) - 1.0) < 1e-6
+
+
+def test_mixed_thick_restart(golden):
+    """Thick restart (the 3 lowest Ritz vectors and their sigma kept) reaches the
+    same energy in no more sigma builds than the reference's collapse restart."""
+    if "energy" not in golden:
+        pytest.skip("fixture has no Davidson result")
+    ctx = gpu_ctx(golden)
+    W0 = np.zeros(ctx.n)
+    W0[0] = 1.0
+    e1, _, t1, tt1 = ctx.davidson(W0, 1000, 10, 1e-5, precision=sbd_b200.MIXED)
+    e3, W3, t3, tt3 = ctx.davidson(W0, 1000, 10, 1e-5, precision=sbd_b200.MIXED, restart_keep=3)
+    assert abs(e3 - float(golden["energy"])) < 1e-6
+    assert tt3[-1] < 1e-5
+    assert len(t3) <= len(t1)
