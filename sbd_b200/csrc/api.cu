@@ -208,12 +208,18 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
       TH[j] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
     }
   int kept = 0;  // basis vectors (with their sigma) carried into the next cycle
+  // With Ritz vectors carried across restarts in FP32, one classical
+  // Gram-Schmidt pass leaves the basis drifting out of orthogonality over the
+  // cycles (the projected problem then loses its meaning); a second pass keeps
+  // it orthonormal to FP32 rounding.  The collapse restart keeps one pass.
+  const int gs_passes = keep > 1 ? 2 : 1;
   auto add_correction = [&](int into, double e0) {
     sbdgpu::precondition(R, c->hii, e0, eps_reg, X, n, st);
-    for (int kb = 0; kb < into; kb++) {
-      double olap = sbdgpu::dot_f(c, C[kb], X, C[kb], n);  // <X|C_kb> with X in FP64
-      sbdgpu::axpy_df(X, C[kb], -olap, n, st);
-    }
+    for (int pass = 0; pass < gs_passes; pass++)
+      for (int kb = 0; kb < into; kb++) {
+        double olap = sbdgpu::dot_f(c, C[kb], X, C[kb], n);  // <X|C_kb> with X in FP64
+        sbdgpu::axpy_df(X, C[kb], -olap, n, st);
+      }
     double nc = std::sqrt(sbdgpu::dot(c, X, X, n));
     sbdgpu::scale(X, 1.0 / nc, n, st);
     sbdgpu::convert(X, C[into], n, st);
