@@ -118,6 +118,19 @@ def profiled_traffic_per_det():
     return None
 
 
+def profiled_spmv_traffic():
+    """DRAM bytes of one stored-Hamiltonian product launch at the
+    245,025-determinant case, from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "spmv_kernel_c0_L12_4e_full.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def table_stats(ctx):
     st = {}
     for spin in (0, 1):
@@ -276,6 +289,47 @@ def time_to_e0(ctx, args):
             "note": "wall-clock seconds (one sigma per step dominates); plain time prorated by steps"}
 
 
+def method1_block(args, dev, hbm_peak, peak_kind):
+    """Method 1 (stored Hamiltonian, CSR SpMV) where it fits one GPU: the
+    245,025-determinant full-space case (norb 12, 4a/4b; 349M stored elements,
+    4.2 GB, larger than L2).  At 144M determinants the stored elements would
+    take ~11 TB."""
+    import torch
+    import sbd_b200
+    from sbd_b200 import synth
+    ints, ne, strs = synth.make_workload("c0_L12_4e_full", seed=0)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    n = ctx.n
+    C = torch.randn(n, dtype=torch.float64, device=f"cuda:{dev}",
+                    generator=torch.Generator(device=f"cuda:{dev}").manual_seed(2))
+    C /= torch.linalg.norm(C)
+    S = torch.empty_like(C)
+    fly = []
+    for i in range(args.warmup + args.steps):
+        ctx.sigma_device(C.data_ptr(), S.data_ptr())
+        if i >= args.warmup:
+            fly.append(ctx.last_sigma_ms()[3])
+    nnz = ctx.store_hamiltonian()
+    spmv, tot = [], []
+    for i in range(args.warmup + args.steps):
+        ctx.sigma_device(C.data_ptr(), S.data_ptr())
+        if i >= args.warmup:
+            ms = ctx.last_sigma_ms()
+            spmv.append(ms[0])
+            tot.append(ms[3])
+    torch.cuda.synchronize()
+    ctx.close()
+    k_ms = sum(spmv) / len(spmv)
+    bytes_per = 12.0 * nnz + 8.0 * (n + 1) + 24.0 * n
+    achieved = bytes_per / (k_ms * 1e-3) / 1e9
+    return {"workload": "c0_L12_4e_full", "determinants": n, "stored_elements": nnz,
+            "sigma_per_s": 1000.0 * len(tot) / sum(tot), "on_the_fly_sigma_per_s": 1000.0 * len(fly) / sum(fly),
+            "roofline": {"bound": "hbm", "kernel": "spmv_kernel (stored Hamiltonian)", "achieved": achieved,
+                         "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_kind,
+                         "algorithmic_bytes": bytes_per, "traffic": profiled_spmv_traffic()},
+            "note": "12 bytes per stored element (uint32 ket, FP64 value) + row offsets + hii, C, sigma"}
+
+
 def run_gpu(args):
     import torch
     import sbd_b200
@@ -395,6 +449,8 @@ def run_gpu(args):
     }
     if args.time_to_e0:
         line["time_to_e0"] = time_to_e0(ctx, args)
+    if not args.no_method1:
+        line["method1_stored"] = method1_block(args, dev, hbm_peak, peak_kind)
     if not args.no_cpu_baseline:
         try:
             rs = RefSampler(ints, ne, strs)
@@ -422,6 +478,7 @@ def main():
     ap.add_argument("--traffic", type=float, default=None, help="ncu DRAM bytes per launch of the dominant kernel")
     ap.add_argument("--workload", default=WORKLOAD, help="named workload (smaller ones for profiling captures)")
     ap.add_argument("--time-to-e0", action="store_true", help="also time Davidson to E0 within 1e-6 Eh")
+    ap.add_argument("--no-method1", action="store_true", help="skip the stored-Hamiltonian (method 1) block")
     ap.add_argument("--e0-tol", type=float, default=1e-7, help="residual target of the FP64 reference run")
     ap.add_argument("--mixed-tol", type=float, default=1e-4, help="residual target of the mixed run")
     args = ap.parse_args()

@@ -115,6 +115,21 @@ int sbdgpu_sigma_device(sbdgpu_ctx* ctx, const double* dC, double* dsigma, int p
  * GPU race.  Same result as sbdgpu_sigma_device, FP64 only. */
 int sbdgpu_sigma_device_noalloc(sbdgpu_ctx* ctx, const double* dC, double* dsigma);
 
+/* Method 1 (--method 1): build the Hamiltonian's off-diagonal elements once
+ * and keep them in device memory, CSR by bra determinant (4-byte ket index and
+ * FP64 value per element, 12 bytes); every later FP64 sigma of this context,
+ * the ones inside sbdgpu_davidson included, is then a sparse product with it.
+ * Replaces makeQCham (chemistry/tpb/qcham.h:10-312), which stores the same
+ * elements as (bra, ket, Hij) triplets, and the stored mult
+ * (chemistry/tpb/mult.h:13-123).  FP32 and the no-allocation sigma keep the
+ * on-the-fly build.  nnz (out, may be NULL): elements stored.
+ * SBDGPU_ERR_LIMIT when the elements do not fit in free device memory (with
+ * 1 GiB to spare) or na*nb >= 2^32. */
+int sbdgpu_store_hamiltonian(sbdgpu_ctx* ctx, uint64_t* nnz);
+
+/* Frees the stored Hamiltonian; later sigma builds are on the fly again. */
+int sbdgpu_release_hamiltonian(sbdgpu_ctx* ctx);
+
 /* Restarted Davidson for the lowest root, the reference algorithm of
  * chemistry/tpb/davidson.h:661-923 (block <= max_nb, collapse restart,
  * diagonal preconditioner with eps_reg = 1e-12, modified Gram-Schmidt,

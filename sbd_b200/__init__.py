@@ -26,7 +26,7 @@ EXPORTS = [
     "sbdgpu_create", "sbdgpu_build_tables", "sbdgpu_table_sizes", "sbdgpu_get_tables", "sbdgpu_diag",
     "sbdgpu_sigma", "sbdgpu_sigma_device", "sbdgpu_davidson", "sbdgpu_rdm", "sbdgpu_occupation",
     "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
-    "sbdgpu_sigma_device_noalloc",
+    "sbdgpu_sigma_device_noalloc", "sbdgpu_store_hamiltonian", "sbdgpu_release_hamiltonian",
 ]
 
 
@@ -62,6 +62,8 @@ def lib():
         L.sbdgpu_sigma_device_noalloc.argtypes = [_vp, _vp, _vp]
         L.sbdgpu_davidson.argtypes = [_vp, ctypes.POINTER(Opts), _dp, _dp, _dp, _dp, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_store_hamiltonian.argtypes = [_vp, _u64p]
+        L.sbdgpu_release_hamiltonian.argtypes = [_vp]
         L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
         L.sbdgpu_occupation.argtypes = [_vp, _dp, _dp]
         L.sbdgpu_alpha_weights.argtypes = [_vp, _dp, _dp]
@@ -142,6 +144,17 @@ class Context:
         (scratch in a fixed 12 MiB device array; at most 524,288 determinants;
         the set-up, tables() and hii(), must have run first)."""
         self._check(lib().sbdgpu_sigma_device_noalloc(self._h, _vp(dC_ptr), _vp(dS_ptr)))
+
+    def store_hamiltonian(self) -> int:
+        """Method 1: keep the Hamiltonian's off-diagonal elements on the device
+        (makeQCham, chemistry/tpb/qcham.h:10-312); later FP64 sigma builds,
+        those of davidson() included, use them.  Returns the element count."""
+        nnz = np.zeros(1, dtype=np.uint64)
+        self._check(lib().sbdgpu_store_hamiltonian(self._h, _p(nnz, _u64p)))
+        return int(nnz[0])
+
+    def release_hamiltonian(self) -> None:
+        self._check(lib().sbdgpu_release_hamiltonian(self._h))
 
     def last_sigma_ms(self):
         a = (ctypes.c_float * 5)()

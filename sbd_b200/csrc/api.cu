@@ -372,6 +372,20 @@ int sbdgpu_build_tables(sbdgpu_ctx* c) {
   return guarded(c, [&] { sbdgpu::build_tables(c); });
 }
 
+int sbdgpu_store_hamiltonian(sbdgpu_ctx* c, uint64_t* nnz) {
+  return guarded(c, [&] {
+    sbdgpu::store_hamiltonian(c);
+    if (nnz) *nnz = c->hs_nnz;
+  });
+}
+
+int sbdgpu_release_hamiltonian(sbdgpu_ctx* c) {
+  return guarded(c, [&] {
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+    sbdgpu::release_hamiltonian(c);
+  });
+}
+
 int sbdgpu_table_sizes(sbdgpu_ctx* c, int spin, uint64_t* ns, uint64_t* nd) {
   return guarded(c, [&] {
     if (spin < 0 || spin > 1) throw Error{SBDGPU_ERR_ARG, "spin must be 0 or 1"};
@@ -597,6 +611,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  sbdgpu::release_hamiltonian(c);
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);

@@ -86,6 +86,12 @@ struct sbdgpu_ctx {
   int* tc_err = nullptr;
   void* ct16 = nullptr;  // BF16 copy of C^T, rows padded to 64 (tensor-core path)
   sbdgpu::SpinTables tab[2];
+  // stored Hamiltonian (method 1): off-diagonal elements, CSR by bra determinant
+  int64_t* hs_row = nullptr;   // [N+1]
+  uint32_t* hs_col = nullptr;  // ket determinant ja*nb + jb
+  double* hs_val = nullptr;
+  uint64_t hs_nnz = 0;
+  bool stored = false;
   bool tables_ready = false;
   bool hii_ready = false;
   // scratch vectors (FP64, N each), allocated on first use
@@ -140,6 +146,11 @@ bool tc_ab_supported(const sbdgpu_ctx* c);
 void build_tc_buckets(sbdgpu_ctx* c);
 void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out);
 int tc_error(sbdgpu_ctx* c);
+
+// stored.cu
+void store_hamiltonian(sbdgpu_ctx* c);
+void release_hamiltonian(sbdgpu_ctx* c);
+void spmv_stored(sbdgpu_ctx* c, const double* C, double* S);
 
 // sigma.cu
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);

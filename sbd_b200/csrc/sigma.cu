@@ -270,6 +270,10 @@ void sigma_launch(sbdgpu_ctx* c, const T* C, T* S, T* ct, T* st, const T* ja, co
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S) {
   build_tables(c);
   compute_hii(c);
+  if (c->stored) {  // method 1: the product with the stored Hamiltonian
+    spmv_stored(c, C, S);
+    return;
+  }
   ensure_scratch(c);
   sigma_launch<double>(c, C, S, c->ct, c->st, c->ja, c->jb, c->vf, true);
 }

@@ -447,17 +447,24 @@ inline void diag(const MPI_Comm& comm, const SBD& sbd_data, const FCIDump& fcidu
   }
   std::cout << " Elapsed time for init " << elapsed_since(t_init) << " (sec) " << std::endl;
 
-  if (sbd_data.method != 0)
+  auto t_diag = std::chrono::high_resolution_clock::now();
+  if (sbd_data.method == 1) {
+    // method 1 (sbdiag.h:264-300): store the Hamiltonian, then Davidson on it
+    auto t_mkham = std::chrono::high_resolution_clock::now();
+    uint64_t nnz = 0;
+    g.check(sbdgpu_store_hamiltonian(g.c, &nnz), "sbdgpu_store_hamiltonian");
+    std::cout << " Elapsed time for make Hamiltonian " << elapsed_since(t_mkham) << " (sec) " << std::endl;
+  } else if (sbd_data.method != 0) {
     std::cout << " method " << sbd_data.method
               << ": the GPU path builds H*C on the fly (method 0); results are the same" << std::endl;
-  auto t_diag = std::chrono::high_resolution_clock::now();
+  }
   sbdgpu_opts o{sbd_data.max_it, sbd_data.max_nb, sbd_data.eps, sbd_data.max_time, sbd_data.precision, 1, 0};
   double e = 0.0;
   int steps = 0;
+  auto t_dav = std::chrono::high_resolution_clock::now();
   g.check(sbdgpu_davidson(g.c, &o, W.data(), &e, nullptr, nullptr, 0, &steps), "sbdgpu_davidson");
-  double td = elapsed_since(t_diag);
-  std::cout << " Elapsed time for davidson " << td << " (sec) " << std::endl;
-  std::cout << " Elapsed time for diagonalization " << td << " (sec) " << std::endl;
+  std::cout << " Elapsed time for davidson " << elapsed_since(t_dav) << " (sec) " << std::endl;
+  std::cout << " Elapsed time for diagonalization " << elapsed_since(t_diag) << " (sec) " << std::endl;
   std::cout.precision(16);
   std::cout << " Energy = " << e << std::endl;
   energy = e;
