@@ -72,6 +72,8 @@ class Reference:
             lib.sbdref_carryover.restype = ctypes.c_size_t
             lib.sbdref_carryover.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, _u64p, _dp]
             lib.sbdref_max_threads.restype = ctypes.c_int
+            lib.sbdref_save_wavefunction.argtypes = [vp, ctypes.c_char_p, _dp]
+            lib.sbdref_load_wavefunction.argtypes = [vp, ctypes.c_char_p, _dp]
             cls._lib = lib
         return cls._lib
 
@@ -158,6 +160,17 @@ class Reference:
         w = np.zeros(1)
         n = self.lib().sbdref_carryover(self.h, _ptr(W, _dp), ratio, threshold, _ptr(out, _u64p), _ptr(w, _dp))
         return out[:n], float(w[0])
+
+    def save_wavefunction(self, prefix: str, W: np.ndarray) -> None:
+        """SaveWavefunction (restart.h:20-66): writes prefix + '000000'."""
+        W = np.ascontiguousarray(W, dtype=np.float64).ravel()
+        self.lib().sbdref_save_wavefunction(self.h, prefix.encode(), _ptr(W, _dp))
+
+    def load_wavefunction(self, prefix: str) -> np.ndarray:
+        """LoadWavefunction (restart.h:414-658) onto this handle's basis."""
+        out = np.zeros(self.na * self.nb)
+        self.lib().sbdref_load_wavefunction(self.h, prefix.encode(), _ptr(out, _dp))
+        return out
 
 
 _TRACE = re.compile(r"Davidson iteration (\d+)\.(\d+) \(tol=([^)]+)\):\s*(\S+)")

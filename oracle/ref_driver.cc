@@ -19,6 +19,9 @@
  *   sbdref_correlation Correlation (chemistry/tpb/correlation.h:194-443)
  *   sbdref_occupation  OccupationDensity (chemistry/tpb/occupation.h:10-95)
  *   sbdref_carryover   CarryOverAlphaDet (chemistry/tpb/rdmat.h:159-231)
+ *   sbdref_save_wavefunction / sbdref_load_wavefunction
+ *                      SaveWavefunction / LoadWavefunction (chemistry/tpb/restart.h:20-66,
+ *                      414-658), the load mapping a saved basis onto this handle's
  */
 #include <omp.h>
 // the same standard headers the reference sample driver includes before sbd.h
@@ -293,6 +296,22 @@ size_t sbdref_carryover(void* hp, const double* W, double ratio, double threshol
   if (weight) *weight = tw;
   for (size_t i = 0; i < rdet.size(); i++) out[i] = pack_string(rdet[i], h->bit_length, h->L);
   return rdet.size();
+}
+
+/* Writes W (this handle's basis) with the reference's SaveWavefunction. */
+void sbdref_save_wavefunction(void* hp, const char* file, const double* W) {
+  RefHandle* h = static_cast<RefHandle*>(hp);
+  std::vector<double> w(W, W + h->adet.size() * h->bdet.size());
+  sbd::SaveWavefunction(std::string(file), h->adet, h->bdet, 1, 1, 0, 0, 0, w);
+}
+
+/* Reads a saved wavefunction onto this handle's basis (string lookup, then
+ * normalisation) with the reference's LoadWavefunction. */
+void sbdref_load_wavefunction(void* hp, const char* file, double* W) {
+  RefHandle* h = static_cast<RefHandle*>(hp);
+  std::vector<double> w(h->adet.size() * h->bdet.size(), 0.0);
+  sbd::LoadWavefunction(std::string(file), h->adet, h->bdet, 1, 1, 0, 0, 0, w);
+  for (size_t i = 0; i < w.size(); i++) W[i] = w[i];
 }
 
 }  // extern "C"
