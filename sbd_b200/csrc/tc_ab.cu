@@ -38,8 +38,9 @@ constexpr int kTcChunks = kTcK / 8;             // 16-byte core-matrix columns a
 constexpr uint32_t kLBO = 128;                  // bytes between K-adjacent core matrices
 constexpr uint32_t kSBO = kTcChunks * 128;      // bytes between 8-row groups
 constexpr int kTcMaxMTiles = 8;                 // 8 x 64 = 512 TMEM columns
-constexpr int kGStride = kTcN + 1;              // padded epilogue staging row
+constexpr int kGStride = kTcN + 4;  // epilogue staging row: 16-byte stores of 8 lanes hit distinct banks
 constexpr long long kSpinLimit = 1ll << 26;
+constexpr int kEntPerMt = 4;  // bucket entries per thread and M tile prefetched into registers
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -128,6 +129,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   __shared__ int s_jb[kTcK];
   __shared__ int s_rs[kTcK];
   __shared__ float s_sb[kTcK];
+  __shared__ int64_t s_bo[kTcMaxMTiles + 1];
   __shared__ uint32_t s_tmem;
   __shared__ __align__(8) uint64_t s_mbar;
   __shared__ int s_fail;
@@ -190,15 +192,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
       }
       __syncthreads();
       load_b(0, 0);
-      // A[m][t] = sb_t (pq_m | rs_t); (pq|rs) is symmetric, so row rs_t of Vf is read
-      for (int idx = tid; idx < Mrows * kTcK; idx += kTcThreads) {
-        int t = idx / Mrows, m = idx - t * Mrows;
-        int rs = s_rs[t];
-        float v = (rs >= 0 && m < a.P) ? s_sb[t] * a.vf[(size_t)rs * a.P + m] : 0.f;
-        *reinterpret_cast<__nv_bfloat16*>(A + kmajor_offset(m, t)) = __float2bfloat16_rn(v);
+      // A[m][t] = sb_t (pq_m | rs_t); (pq|rs) is symmetric, so row rs_t of Vf is
+      // read; eight independent loads in flight per thread
+      for (int base = 0; base < Mrows * kTcK; base += 8 * kTcThreads) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int idx = base + u * kTcThreads + tid;
+          const int t = idx / Mrows, m = idx - t * Mrows;
+          const int rs = idx < Mrows * kTcK ? s_rs[t] : -1;
+          v[u] = (rs >= 0 && m < a.P) ? __ldg(&a.vf[(size_t)rs * a.P + m]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int idx = base + u * kTcThreads + tid;
+          if (idx < Mrows * kTcK) {
+            const int t = idx / Mrows, m = idx - t * Mrows;
+            *reinterpret_cast<__nv_bfloat16*>(A + kmajor_offset(m, t)) = __float2bfloat16_rn(s_sb[t] * v[u]);
+          }
+        }
       }
+      // bucket offsets of the next tile's M tiles, fetched one tile ahead
+      int64_t bo_next = tid <= a.mtiles ? __ldg(&a.bk_off[tid]) : 0;
       for (int tile = 0; tile < ntiles && !s_fail; tile++) {
         const int buf = tile & 1;
+        // this tile's bucket offsets (the previous tile's epilogue ended with a
+        // barrier, so nobody still reads the old ones)
+        if (tid <= a.mtiles) s_bo[tid] = bo_next;
         asm volatile("cp.async.wait_group 0;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -215,6 +235,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
         }
         // the other buffer was read by the previous tile's MMAs, which completed
         if (tile + 1 < ntiles) load_b(tile + 1, buf ^ 1);
+        if (tile + 1 < ntiles && tid <= a.mtiles) bo_next = __ldg(&a.bk_off[(size_t)(tile + 1) * a.mtiles + tid]);
+        // this tile's bucket entries, loaded while the MMAs run: entry
+        // e = s_bo[mt] + tid + u * kTcThreads of M tile mt in register [mt][u]
+        uint32_t ent[kTcMaxMTiles][kEntPerMt];
+#pragma unroll
+        for (int mt = 0; mt < kTcMaxMTiles; mt++)
+#pragma unroll
+          for (int u = 0; u < kEntPerMt; u++) {
+            const int64_t e = (mt < a.mtiles ? s_bo[mt] : 0) + tid + (int64_t)u * kTcThreads;
+            ent[mt][u] = (mt < a.mtiles && e < s_bo[mt + 1]) ? __ldg(&a.bk_ent[e]) : 0xFFFFFFFFu;
+          }
         if (!mbar_wait(mbar, phase)) {
           if (tid == 0) atomicExch(a.err, 1);
           s_fail = 1;
@@ -223,23 +254,36 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
         __syncthreads();
         if (s_fail) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        for (int mt = 0; mt < a.mtiles; mt++) {
+#pragma unroll
+        for (int mt = 0; mt < kTcMaxMTiles; mt++) {
+          if (mt >= a.mtiles) break;
           // TMEM lanes 32q..32q+31 hold rows pq = 128 mt + 32 q + lane; columns split by half
-          float v[16];
+          float v0[16], v1[16];
+          const uint32_t trow = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(mt * kTcN + 32 * half);
+          tmem_ld16(trow, v0);
+          tmem_ld16(trow + 16u, v1);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          float4* grow = reinterpret_cast<float4*>(G + (32 * quarter + lane) * kGStride + 32 * half);
 #pragma unroll
-          for (int c = 0; c < 2; c++) {
-            const int col = 32 * half + 16 * c;
-            tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(mt * kTcN + col), v);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int i = 0; i < 16; i++) G[(32 * quarter + lane) * kGStride + col + i] = v[i];
+          for (int i = 0; i < 4; i++) {
+            grow[i] = make_float4(v0[4 * i], v0[4 * i + 1], v0[4 * i + 2], v0[4 * i + 3]);
+            grow[4 + i] = make_float4(v1[4 * i], v1[4 * i + 1], v1[4 * i + 2], v1[4 * i + 3]);
           }
           __syncthreads();
-          const int64_t e0 = a.bk_off[(size_t)tile * a.mtiles + mt], e1 = a.bk_off[(size_t)tile * a.mtiles + mt + 1];
-          for (int64_t e = e0 + tid; e < e1; e += kTcThreads) {
-            uint32_t en = a.bk_ent[e];
-            int jl = en & 63u, pl = (en >> 6) & 127u, ia = (int)(en >> 14);
-            float g = G[pl * kGStride + jl];
+#pragma unroll
+          for (int u = 0; u < kEntPerMt; u++) {
+            const uint32_t en = ent[mt][u];
+            if (en != 0xFFFFFFFFu) {
+              const int jl = en & 63u, pl = (en >> 6) & 127u, ia = (int)(en >> 14);
+              const float g = G[pl * kGStride + jl];
+              atomicAdd(&sig[ia], (en & (1u << 13)) ? -g : g);
+            }
+          }
+          // entries beyond the prefetched ones
+          for (int64_t e = s_bo[mt] + tid + (int64_t)kEntPerMt * kTcThreads; e < s_bo[mt + 1]; e += kTcThreads) {
+            const uint32_t en = __ldg(&a.bk_ent[e]);
+            const int jl = en & 63u, pl = (en >> 6) & 127u, ia = (int)(en >> 14);
+            const float g = G[pl * kGStride + jl];
             atomicAdd(&sig[ia], (en & (1u << 13)) ? -g : g);
           }
           __syncthreads();
@@ -275,7 +319,8 @@ size_t tc_smem_bytes(int mtiles, size_t na) {
 
 bool tc_ab_supported(const sbdgpu_ctx* c) {
   int mtiles = (c->P + 127) / 128;
-  return mtiles <= kTcMaxMTiles && c->na <= (1 << 18) && tc_smem_bytes(mtiles, c->na) <= 225 * 1024;
+  // na < 2^18: an entry of all ones (ia = 2^18 - 1) is the empty-register marker
+  return mtiles <= kTcMaxMTiles && c->na < (1 << 18) && tc_smem_bytes(mtiles, c->na) <= 225 * 1024;
 }
 
 // Alpha singles bucketed by (tile of 64 source strings ja, M tile of 128 pq).
