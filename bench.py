@@ -260,7 +260,11 @@ def time_to_e0(ctx, args):
     energy.  Plain time-to-E0 = time of the first step whose Ritz value is
     within 1e-6 Eh of it (steps cost the same: one sigma each); mixed
     time-to-E0 = the whole mixed run including its FP64 refinement sigma, whose
-    energy must land within 1e-6 Eh."""
+    energy must land within 1e-6 Eh.  The plain run's first step within 1e-6 Eh
+    is found in hindsight; the mixed runs stop on a residual norm they can check
+    at run time (default 1e-3, where the energy error, about 0.16 r^2 on this
+    system, is ~2e-7 Eh), and each one's error against the FP64 energy is
+    reported with a flag for the 1e-6 Eh bound."""
     import sbd_b200
     W0 = np.zeros(ctx.n)
     W0[0] = 1.0
@@ -286,6 +290,9 @@ def time_to_e0(ctx, args):
             "plain_steps_total": len(te), "plain_steps_to_1e-6": k, "plain_s_to_1e-6": t_plain,
             "plain_final_residual": float(tt[-1]), "mixed_steps": len(tm), "mixed_s": t_mixed,
             "mixed_final_residual": float(ttm[-1]), "speedup": t_plain / t_mixed,
+            "within_1e-6": {"mixed": abs(e_mix - e_ref) < 1e-6, "mixed_thick3": abs(e_mk - e_ref) < 1e-6,
+                            "mixed_tc": abs(e_tc - e_ref) < 1e-6},
+            "mixed_tol": args.mixed_tol,
             "note": "wall-clock seconds (one sigma per step dominates); plain time prorated by steps"}
 
 
@@ -480,7 +487,7 @@ def main():
     ap.add_argument("--time-to-e0", action="store_true", help="also time Davidson to E0 within 1e-6 Eh")
     ap.add_argument("--no-method1", action="store_true", help="skip the stored-Hamiltonian (method 1) block")
     ap.add_argument("--e0-tol", type=float, default=1e-7, help="residual target of the FP64 reference run")
-    ap.add_argument("--mixed-tol", type=float, default=1e-4, help="residual target of the mixed run")
+    ap.add_argument("--mixed-tol", type=float, default=1e-3, help="residual target of the mixed runs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
