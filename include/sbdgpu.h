@@ -115,6 +115,22 @@ int sbdgpu_sigma_device(sbdgpu_ctx* ctx, const double* dC, double* dsigma, int p
  * GPU race.  Same result as sbdgpu_sigma_device, FP64 only. */
 int sbdgpu_sigma_device_noalloc(sbdgpu_ctx* ctx, const double* dC, double* dsigma);
 
+/* Block Davidson for the nroots lowest roots, FP64 (an extension: the
+ * reference's Davidson, chemistry/tpb/davidson.h:661-923, follows the lowest
+ * root only).  Each cycle adds one diagonally preconditioned correction per
+ * unconverged root; when the basis would pass opts->max_nb vectors
+ * (2*nroots <= max_nb <= 32) it collapses to the Ritz vectors.  Stops when
+ * every residual norm is below opts->eps, after opts->max_it cycles, or at
+ * opts->max_time seconds.
+ *   W         [nroots][na*nb], reference convention.  In: initial vectors, or
+ *             all zeros for the nroots lowest-H_ii determinants.  Out: the
+ *             normalised Ritz vectors.
+ *   energies  out [nroots]: Ritz values, ascending
+ *   resid     out [nroots] (may be NULL): residual norms
+ *   n_iter, n_sigma  out (may be NULL): cycles, sigma builds */
+int sbdgpu_davidson_roots(sbdgpu_ctx* ctx, const sbdgpu_opts* opts, int nroots, double* W, double* energies,
+                          double* resid, int* n_iter, int* n_sigma);
+
 /* Method 1 (--method 1): build the Hamiltonian's off-diagonal elements once
  * and keep them in device memory, CSR by bra determinant (4-byte ket index and
  * FP64 value per element, 12 bytes); every later FP64 sigma of this context,

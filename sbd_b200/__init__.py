@@ -27,6 +27,7 @@ EXPORTS = [
     "sbdgpu_sigma", "sbdgpu_sigma_device", "sbdgpu_davidson", "sbdgpu_rdm", "sbdgpu_occupation",
     "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
     "sbdgpu_sigma_device_noalloc", "sbdgpu_store_hamiltonian", "sbdgpu_release_hamiltonian",
+    "sbdgpu_davidson_roots",
 ]
 
 
@@ -62,6 +63,8 @@ def lib():
         L.sbdgpu_sigma_device_noalloc.argtypes = [_vp, _vp, _vp]
         L.sbdgpu_davidson.argtypes = [_vp, ctypes.POINTER(Opts), _dp, _dp, _dp, _dp, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_davidson_roots.argtypes = [_vp, ctypes.POINTER(Opts), ctypes.c_int, _dp, _dp, _dp,
+                                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_store_hamiltonian.argtypes = [_vp, _u64p]
         L.sbdgpu_release_hamiltonian.argtypes = [_vp]
         L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
@@ -144,6 +147,20 @@ class Context:
         (scratch in a fixed 12 MiB device array; at most 524,288 determinants;
         the set-up, tables() and hii(), must have run first)."""
         self._check(lib().sbdgpu_sigma_device_noalloc(self._h, _vp(dC_ptr), _vp(dS_ptr)))
+
+    def davidson_roots(self, nroots: int, max_it: int, max_nb: int, eps: float, W0: np.ndarray | None = None,
+                       max_time: float = 86400.0, verbose: int = 0):
+        """Block Davidson for the nroots lowest roots (FP64).  Returns
+        (energies[nroots], W[nroots, n], residual norms, cycles, sigma builds)."""
+        W = np.zeros((nroots, self.n)) if W0 is None else np.ascontiguousarray(W0, dtype=np.float64).reshape(
+            nroots, self.n).copy()
+        o = Opts(max_it, max_nb, eps, max_time, FP64, verbose, 0)
+        e = np.zeros(nroots)
+        r = np.zeros(nroots)
+        it, ns = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().sbdgpu_davidson_roots(self._h, ctypes.byref(o), nroots, _p(W, _dp), _p(e, _dp), _p(r, _dp),
+                                                ctypes.byref(it), ctypes.byref(ns)))
+        return e, W, r, it.value, ns.value
 
     def store_hamiltonian(self) -> int:
         """Method 1: keep the Hamiltonian's off-diagonal elements on the device

@@ -575,6 +575,11 @@ int sbdgpu_davidson(sbdgpu_ctx* c, const sbdgpu_opts* o, double* Wh, double* ene
   });
 }
 
+int sbdgpu_davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, double* W, double* energies,
+                          double* resid, int* n_iter, int* n_sigma) {
+  return guarded(c, [&] { sbdgpu::davidson_roots(c, o, nroots, W, energies, resid, n_iter, n_sigma); });
+}
+
 int sbdgpu_rdm(sbdgpu_ctx* c, const double* Wh, double* one, double* two) {
   return guarded(c, [&] {
     if (!Wh || !one || !two) throw Error{SBDGPU_ERR_ARG, "null argument"};

@@ -152,6 +152,10 @@ void store_hamiltonian(sbdgpu_ctx* c);
 void release_hamiltonian(sbdgpu_ctx* c);
 void spmv_stored(sbdgpu_ctx* c, const double* C, double* S);
 
+// roots.cu
+void davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, double* Wh, double* energies, double* resid,
+                    int* n_iter, int* n_sigma);
+
 // sigma.cu
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);
 void sigma_fp64_prepared(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st);
