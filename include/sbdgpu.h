@@ -181,6 +181,14 @@ int sbdgpu_alpha_weights(sbdgpu_ctx* ctx, const double* W, double* D);
  * prints wall-clock timers (chemistry/tpb/mult.h:435-446, 619-646). */
 int sbdgpu_last_sigma_ms(sbdgpu_ctx* ctx, float* ms5);
 
+/* Diagnostic of the bounded wait that the tensor-core kernel uses on its
+ * MMA-completion barrier (no reference counterpart).  Launches one warp that
+ * waits on a barrier nobody arrives on, polling at most spin_limit times, and
+ * one that arrives first.  status[0] = 1 when the first wait gave up (the
+ * expected outcome), status[1] = 0 when the second completed.  The context
+ * stays usable either way. */
+int sbdgpu_wait_selftest(sbdgpu_ctx* ctx, long long spin_limit, int* status);
+
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);
 void sbdgpu_destroy(sbdgpu_ctx* ctx);
 

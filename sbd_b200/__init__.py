@@ -27,7 +27,7 @@ EXPORTS = [
     "sbdgpu_sigma", "sbdgpu_sigma_device", "sbdgpu_davidson", "sbdgpu_rdm", "sbdgpu_occupation",
     "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
     "sbdgpu_sigma_device_noalloc", "sbdgpu_store_hamiltonian", "sbdgpu_release_hamiltonian",
-    "sbdgpu_davidson_roots",
+    "sbdgpu_davidson_roots", "sbdgpu_wait_selftest",
 ]
 
 
@@ -65,6 +65,7 @@ def lib():
                                       ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_davidson_roots.argtypes = [_vp, ctypes.POINTER(Opts), ctypes.c_int, _dp, _dp, _dp,
                                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_wait_selftest.argtypes = [_vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_store_hamiltonian.argtypes = [_vp, _u64p]
         L.sbdgpu_release_hamiltonian.argtypes = [_vp]
         L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
@@ -161,6 +162,13 @@ class Context:
         self._check(lib().sbdgpu_davidson_roots(self._h, ctypes.byref(o), nroots, _p(W, _dp), _p(e, _dp), _p(r, _dp),
                                                 ctypes.byref(it), ctypes.byref(ns)))
         return e, W, r, it.value, ns.value
+
+    def wait_selftest(self, spin_limit: int = 4096):
+        """(first wait timed out, second wait timed out) of the bounded
+        mbarrier-wait diagnostic; (1, 0) is the expected answer."""
+        st = (ctypes.c_int * 2)()
+        self._check(lib().sbdgpu_wait_selftest(self._h, int(spin_limit), st))
+        return int(st[0]), int(st[1])
 
     def store_hamiltonian(self) -> int:
         """Method 1: keep the Hamiltonian's off-diagonal elements on the device

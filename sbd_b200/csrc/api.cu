@@ -580,6 +580,13 @@ int sbdgpu_davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, doubl
   return guarded(c, [&] { sbdgpu::davidson_roots(c, o, nroots, W, energies, resid, n_iter, n_sigma); });
 }
 
+int sbdgpu_wait_selftest(sbdgpu_ctx* c, long long spin_limit, int* status) {
+  return guarded(c, [&] {
+    if (!status || spin_limit < 1) throw Error{SBDGPU_ERR_ARG, "status must be non-null and spin_limit >= 1"};
+    sbdgpu::wait_selftest(c, spin_limit, status);
+  });
+}
+
 int sbdgpu_rdm(sbdgpu_ctx* c, const double* Wh, double* one, double* two) {
   return guarded(c, [&] {
     if (!Wh || !one || !two) throw Error{SBDGPU_ERR_ARG, "null argument"};

@@ -146,6 +146,7 @@ bool tc_ab_supported(const sbdgpu_ctx* c);
 void build_tc_buckets(sbdgpu_ctx* c);
 void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out);
 int tc_error(sbdgpu_ctx* c);
+void wait_selftest(sbdgpu_ctx* c, long long limit, int* status);
 
 // stored.cu
 void store_hamiltonian(sbdgpu_ctx* c);

@@ -81,8 +81,8 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (long long i = 0; i < kSpinLimit; i++) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit = kSpinLimit) {
+  for (long long i = 0; i < limit; i++) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -302,6 +302,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
 
+// The bounded mbarrier wait of tc_ab_kernel on its own: one warp waits for
+// phase 0 of a barrier that expects one arrival; with arrive = 0 nothing
+// arrives, so the wait must give up after `limit` polls and report it.
+__global__ void wait_probe_kernel(long long limit, int arrive, int* timed_out) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t mbar = smem_addr(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (arrive && threadIdx.x == 0)
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(mbar) : "memory");
+  const bool ok = mbar_wait(mbar, 0u, limit);
+  __syncthreads();
+  if (threadIdx.x == 0) *timed_out = ok ? 0 : 1;
+}
+
 __global__ void to_bf16_padded_kernel(const float* __restrict__ in, __nv_bfloat16* __restrict__ out, size_t rows,
                                       size_t cols, size_t cols_pad) {
   size_t n = rows * cols_pad;
@@ -316,6 +334,25 @@ size_t tc_smem_bytes(int mtiles, size_t na) {
 }
 
 }  // namespace
+
+// status[0]: the wait with no arrival timed out (expected 1); status[1]: the
+// wait after one arrival timed out (expected 0)
+void wait_selftest(sbdgpu_ctx* c, long long limit, int* status) {
+  int* d = (int*)dev_alloc(2 * sizeof(int));
+  try {
+    SBD_CUDA(cudaMemsetAsync(d, 0xFF, 2 * sizeof(int), c->stream));
+    wait_probe_kernel<<<1, 32, 0, c->stream>>>(limit, 0, d);
+    SBD_CUDA(cudaGetLastError());
+    wait_probe_kernel<<<1, 32, 0, c->stream>>>(limit, 1, d + 1);
+    SBD_CUDA(cudaGetLastError());
+    SBD_CUDA(cudaMemcpyAsync(status, d, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+  } catch (...) {
+    cudaFree(d);
+    throw;
+  }
+  cudaFree(d);
+}
 
 bool tc_ab_supported(const sbdgpu_ctx* c) {
   int mtiles = (c->P + 127) / 128;

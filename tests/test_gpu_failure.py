@@ -1,0 +1,28 @@
+"""Failure detection on the GPU without a GPU fault: the bounded mbarrier wait
+that the tensor-core kernel uses gives up on a barrier nobody arrives on,
+reports it through a status the host reads, and the context keeps working."""
+import numpy as np
+import pytest
+
+from conftest import load_golden, seeded_vector
+from test_gpu_parity import gpu_ctx
+
+pytestmark = pytest.mark.gpu
+
+
+def test_bounded_wait_gives_up_and_context_survives():
+    g = load_golden("g_L8_3e_full")
+    ctx = gpu_ctx(g)
+    assert ctx.wait_selftest(4096) == (1, 0)
+    assert ctx.wait_selftest(1) == (1, 0)
+    C = seeded_vector(ctx.n, int(g["C_seed"]))
+    r0, r1 = (int(x) for x in g["sigma_rows"])
+    s = ctx.sigma(C)[r0 * ctx.nb:r1 * ctx.nb]
+    assert np.abs(s - g["sigma"]).max() <= 1e-12 * np.abs(g["sigma"]).max()
+
+
+def test_wait_selftest_rejects_bad_limit():
+    import sbd_b200
+    ctx = gpu_ctx(load_golden("g_L8_3e_full"))
+    with pytest.raises(sbd_b200.SbdGpuError, match="spin_limit"):
+        ctx.wait_selftest(0)
