@@ -30,7 +30,9 @@ namespace sbdgpu {
 
 namespace {
 
-constexpr int kTcThreads = 256;  // 8 warps: warp w reads TMEM lane quarter w % 4, column half w / 4
+// 16 warps: warp w reads TMEM lane quarter w % 4 and the column group w / 4
+// (kWarpCols columns) of each accumulator in the epilogue
+constexpr int kTcThreads = 512;
 constexpr int kTcN = 64;         // alpha strings (ja) per tile
 constexpr int kTcK = 80;         // beta singles per K chunk (5 MMA steps of 16)
 constexpr int kTcKSteps = kTcK / 16;
@@ -38,9 +40,11 @@ constexpr int kTcChunks = kTcK / 8;             // 16-byte core-matrix columns a
 constexpr uint32_t kLBO = 128;                  // bytes between K-adjacent core matrices
 constexpr uint32_t kSBO = kTcChunks * 128;      // bytes between 8-row groups
 constexpr int kTcMaxMTiles = 8;                 // 8 x 64 = 512 TMEM columns
+constexpr int kWarpCols = kTcN * 4 / (kTcThreads / 32);  // accumulator columns per warp in the epilogue
+static_assert(kWarpCols % 16 == 0 && kWarpCols >= 16, "epilogue reads 16-column groups");
 constexpr int kGStride = kTcN + 4;  // epilogue staging row: 16-byte stores of 8 lanes hit distinct banks
 constexpr long long kSpinLimit = 1ll << 26;
-constexpr int kEntPerMt = 4;  // bucket entries per thread and M tile prefetched into registers
+constexpr int kEntPerMt = 2;  // bucket entries per thread and M tile prefetched into registers
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   __shared__ int s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, half = warp >> 2;
+  const int quarter = warp & 3, cgroup = warp >> 2;
   const uint32_t mbar = smem_addr(&s_mbar);
   // TMEM columns: a power of two >= 64 per M tile, so small problems leave
   // room for other CTAs on the SM
@@ -257,18 +261,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
 #pragma unroll
         for (int mt = 0; mt < kTcMaxMTiles; mt++) {
           if (mt >= a.mtiles) break;
-          // TMEM lanes 32q..32q+31 hold rows pq = 128 mt + 32 q + lane; columns split by half
-          float v0[16], v1[16];
-          const uint32_t trow = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(mt * kTcN + 32 * half);
-          tmem_ld16(trow, v0);
-          tmem_ld16(trow + 16u, v1);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          float4* grow = reinterpret_cast<float4*>(G + (32 * quarter + lane) * kGStride + 32 * half);
+          // TMEM lanes 32q..32q+31 hold rows pq = 128 mt + 32 q + lane; this
+          // warp stages columns [kWarpCols * cgroup, kWarpCols * (cgroup + 1))
+          float v[kWarpCols];
+          const uint32_t trow =
+              tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(mt * kTcN + kWarpCols * cgroup);
 #pragma unroll
-          for (int i = 0; i < 4; i++) {
-            grow[i] = make_float4(v0[4 * i], v0[4 * i + 1], v0[4 * i + 2], v0[4 * i + 3]);
-            grow[4 + i] = make_float4(v1[4 * i], v1[4 * i + 1], v1[4 * i + 2], v1[4 * i + 3]);
-          }
+          for (int c16 = 0; c16 < kWarpCols / 16; c16++) tmem_ld16(trow + 16u * c16, v + 16 * c16);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          float4* grow = reinterpret_cast<float4*>(G + (32 * quarter + lane) * kGStride + kWarpCols * cgroup);
+#pragma unroll
+          for (int i = 0; i < kWarpCols / 4; i++) grow[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
           __syncthreads();
 #pragma unroll
           for (int u = 0; u < kEntPerMt; u++) {
