@@ -337,6 +337,32 @@ def method1_block(args, dev, hbm_peak, peak_kind):
             "note": "12 bytes per stored element (uint32 ket, FP64 value) + row offsets + hii, C, sigma"}
 
 
+def roots_block(args, dev):
+    """Block Davidson for the lowest args.roots roots (FP64) on the
+    16M-determinant system (norb 26, 6a/6b, 4000 x 4000 strings): wall time,
+    cycles, sigma builds, residual norms, and root 0 against the single-root
+    FP64 Davidson of the same system."""
+    import sbd_b200
+    from sbd_b200 import synth
+    ints, ne, strs = synth.make_workload("c1_L26_6e_4000", seed=0)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    k = args.roots
+    nb = min(32, max(2 * k, 3 * k))
+    t = time.perf_counter()
+    E, W, r, it, ns = ctx.davidson_roots(k, 400, nb, args.roots_tol)
+    t_block = time.perf_counter() - t
+    W0 = np.zeros(ctx.n)
+    W0[0] = 1.0
+    t = time.perf_counter()
+    e1, _, te, _ = ctx.davidson(W0, 200, 10, args.roots_tol)
+    t_one = time.perf_counter() - t
+    ctx.close()
+    return {"workload": "c1_L26_6e_4000", "roots": k, "max_nb": nb, "eps": args.roots_tol, "seconds": t_block,
+            "cycles": it, "sigma_builds": ns, "energies": [float(x) for x in E],
+            "residuals": [float(x) for x in r], "root0_minus_single_root": float(E[0] - e1),
+            "single_root_seconds": t_one, "single_root_steps": len(te)}
+
+
 def run_gpu(args):
     import torch
     import sbd_b200
@@ -458,6 +484,8 @@ def run_gpu(args):
         line["time_to_e0"] = time_to_e0(ctx, args)
     if not args.no_method1:
         line["method1_stored"] = method1_block(args, dev, hbm_peak, peak_kind)
+    if args.roots > 0:
+        line["block_roots"] = roots_block(args, dev)
     if not args.no_cpu_baseline:
         try:
             rs = RefSampler(ints, ne, strs)
@@ -486,6 +514,8 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD, help="named workload (smaller ones for profiling captures)")
     ap.add_argument("--time-to-e0", action="store_true", help="also time Davidson to E0 within 1e-6 Eh")
     ap.add_argument("--no-method1", action="store_true", help="skip the stored-Hamiltonian (method 1) block")
+    ap.add_argument("--roots", type=int, default=0, help="also time block Davidson for this many roots (16M dets)")
+    ap.add_argument("--roots-tol", type=float, default=1e-5, help="residual target of the block Davidson block")
     ap.add_argument("--e0-tol", type=float, default=1e-7, help="residual target of the FP64 reference run")
     ap.add_argument("--mixed-tol", type=float, default=1e-3, help="residual target of the mixed runs")
     args = ap.parse_args()
