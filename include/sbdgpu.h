@@ -63,6 +63,9 @@ typedef struct sbdgpu_opts {
                        the reference's collapse to the lowest Ritz vector
                        (davidson.h:911-915), k > 1 = thick restart with the k lowest,
                        whose sigma vectors are carried over instead of recomputed */
+  int restart_prev; /* mixed precisions only: 1 = also keep the previous step's Ritz
+                       vector at a restart (the "+1" of a GD+k restart), with its
+                       sigma vector; 0 = not (the reference's behaviour) */
 } sbdgpu_opts;
 
 /* Create a context on CUDA device `device` for one alpha x beta product basis

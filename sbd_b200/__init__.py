@@ -38,7 +38,7 @@ class SbdGpuError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("max_it", ctypes.c_int), ("max_nb", ctypes.c_int), ("eps", ctypes.c_double),
                 ("max_time", ctypes.c_double), ("precision", ctypes.c_int), ("verbose", ctypes.c_int),
-                ("restart_keep", ctypes.c_int)]
+                ("restart_keep", ctypes.c_int), ("restart_prev", ctypes.c_int)]
 
 
 _lib = None
@@ -155,7 +155,7 @@ class Context:
         (energies[nroots], W[nroots, n], residual norms, cycles, sigma builds)."""
         W = np.zeros((nroots, self.n)) if W0 is None else np.ascontiguousarray(W0, dtype=np.float64).reshape(
             nroots, self.n).copy()
-        o = Opts(max_it, max_nb, eps, max_time, FP64, verbose, 0)
+        o = Opts(max_it, max_nb, eps, max_time, FP64, verbose, 0, 0)
         e = np.zeros(nroots)
         r = np.zeros(nroots)
         it, ns = ctypes.c_int(0), ctypes.c_int(0)
@@ -187,9 +187,10 @@ class Context:
         return [float(x) for x in a]
 
     def davidson(self, W0: np.ndarray, max_it: int, max_nb: int, eps: float, max_time: float = 86400.0,
-                 precision: int = FP64, verbose: int = 0, max_trace: int = 100000, restart_keep: int = 0):
+                 precision: int = FP64, verbose: int = 0, max_trace: int = 100000, restart_keep: int = 0,
+                 restart_prev: int = 0):
         W = np.ascontiguousarray(W0, dtype=np.float64).ravel().copy()
-        o = Opts(max_it, max_nb, eps, max_time, precision, verbose, restart_keep)
+        o = Opts(max_it, max_nb, eps, max_time, precision, verbose, restart_keep, restart_prev)
         e = ctypes.c_double(0.0)
         te = np.zeros(max_trace)
         tt = np.zeros(max_trace)

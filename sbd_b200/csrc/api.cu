@@ -192,8 +192,14 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
   auto t_start = std::chrono::steady_clock::now();
   int steps = 0;
   bool cont = true;
-  const int keep = std::min(std::max(o->restart_keep, 1), nb - 1);
+  const bool keep_prev = o->restart_prev != 0 && nb > 2;
+  const int keep_ritz = std::min(std::max(o->restart_keep, 1), nb - (keep_prev ? 2 : 1));
+  // basis vectors carried over a restart: the keep_ritz lowest Ritz vectors,
+  // plus the previous step's Ritz vector when keep_prev
+  const int keep = keep_ritz + (keep_prev ? 1 : 0);
   std::vector<float*> T(keep, nullptr), TH(keep, nullptr);
+  std::vector<double> u_last(nb, 0.0);  // Ritz coefficients of the previous step
+  int u_last_len = 0, u_last_cycle = -1;
   struct FreeT {
     std::vector<float*>* a;
     std::vector<float*>* b;
@@ -275,24 +281,57 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
       if (ib < nb - 1) {
         add_correction(ib + 1, E[0]);
       } else if (keep > 1) {
-        // thick restart: the keep lowest Ritz vectors and their sigma vectors
-        std::vector<double> col(nb);
-        for (int j = 0; j < keep; j++) {
-          for (int i = 0; i < nb; i++) col[i] = U[i + nb * j];
-          sbdgpu::lincomb_f(C.data(), col.data(), nb, T[j], n, c);
-          sbdgpu::lincomb_f(HC.data(), col.data(), nb, TH[j], n, c);
+        // thick restart: the keep_ritz lowest Ritz vectors (and the previous
+        // step's Ritz vector, orthonormalised against them in the small space)
+        // with their sigma vectors, as linear combinations of the basis
+        std::vector<std::vector<double>> Q;
+        auto add_col = [&](std::vector<double> y) {
+          for (int pass = 0; pass < 2; pass++)
+            for (const auto& q : Q) {
+              double d = 0.0;
+              for (int i = 0; i < nb; i++) d += q[i] * y[i];
+              for (int i = 0; i < nb; i++) y[i] -= d * q[i];
+            }
+          double nn = 0.0;
+          for (int i = 0; i < nb; i++) nn += y[i] * y[i];
+          nn = std::sqrt(nn);
+          if (nn > 1e-8) {
+            for (int i = 0; i < nb; i++) y[i] /= nn;
+            Q.push_back(std::move(y));
+          }
+        };
+        for (int j = 0; j < keep_ritz; j++) {
+          std::vector<double> y(nb);
+          for (int i = 0; i < nb; i++) y[i] = U[i + nb * j];
+          add_col(std::move(y));
         }
-        for (int j = 0; j < keep; j++) {
+        if (keep_prev && u_last_cycle == it) {
+          std::vector<double> y(nb, 0.0);
+          for (int i = 0; i < u_last_len; i++) y[i] = u_last[i];
+          add_col(std::move(y));
+        }
+        const int kk = (int)Q.size();
+        for (int j = 0; j < kk; j++) {
+          sbdgpu::lincomb_f(C.data(), Q[j].data(), nb, T[j], n, c);
+          sbdgpu::lincomb_f(HC.data(), Q[j].data(), nb, TH[j], n, c);
+        }
+        for (int j = 0; j < kk; j++) {
           std::swap(C[j], T[j]);
           std::swap(HC[j], TH[j]);
         }
-        for (int j = 0; j < keep; j++)
+        for (int j = 0; j < kk; j++)
           for (int i = 0; i <= j; i++) {
             H[i + nb * j] = sbdgpu::dot_f(c, C[i], nullptr, HC[j], n);
             H[j + nb * i] = H[i + nb * j];
           }
-        add_correction(keep, E[0]);
-        kept = keep;
+        add_correction(kk, E[0]);
+        kept = kk;
+      }
+      // this step's Ritz coefficients, kept for the next restart of this cycle
+      if (ib < nb - 1) {
+        for (int i = 0; i <= ib; i++) u_last[i] = U[i];
+        u_last_len = ib + 1;
+        u_last_cycle = it;
       }
       SBD_CUDA(cudaStreamSynchronize(st));
       auto t1 = std::chrono::steady_clock::now();

@@ -458,7 +458,7 @@ inline void diag(const MPI_Comm& comm, const SBD& sbd_data, const FCIDump& fcidu
     std::cout << " method " << sbd_data.method
               << ": the GPU path builds H*C on the fly (method 0); results are the same" << std::endl;
   }
-  sbdgpu_opts o{sbd_data.max_it, sbd_data.max_nb, sbd_data.eps, sbd_data.max_time, sbd_data.precision, 1, 0};
+  sbdgpu_opts o{sbd_data.max_it, sbd_data.max_nb, sbd_data.eps, sbd_data.max_time, sbd_data.precision, 1, 0, 0};
   double e = 0.0;
   int steps = 0;
   auto t_dav = std::chrono::high_resolution_clock::now();

@@ -46,3 +46,11 @@ def test_mixed_thick_restart(golden):
     assert abs(e3 - float(golden["energy"])) < 1e-6
     assert tt3[-1] < 1e-5
     assert len(t3) <= len(t1)
+    # and with the previous step's Ritz vector kept as well (GD+k style)
+    e4, W4, t4, tt4 = ctx.davidson(W0, 1000, 10, 1e-5, precision=sbd_b200.MIXED, restart_keep=3, restart_prev=1)
+    assert abs(e4 - float(golden["energy"])) < 1e-6
+    assert tt4[-1] < 1e-5
+    assert len(t4) <= len(t1)
+    # the previous vector alone with the collapse restart
+    e5, _, t5, tt5 = ctx.davidson(W0, 1000, 10, 1e-5, precision=sbd_b200.MIXED, restart_prev=1)
+    assert abs(e5 - float(golden["energy"])) < 1e-6 and tt5[-1] < 1e-5
