@@ -475,7 +475,10 @@ def run_gpu(args):
         "gpu_launches": LAUNCHES_PER_SIGMA * args.steps * 2,
         "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_kind,
-                     "traffic": traffic},
+                     "traffic": traffic,
+                     "limiter": ("shared-memory pipe: one gathered 8-byte integral per FP64 FMA (ncu at 16M "
+                                 "dets: l1tex 90.8 %, FP64 pipe 24.7 %, profiles/ab_kernel_c1_L26_6e_4000.md)")
+                     if dom == 2 else "L1/L2 streaming of C rows (profiles/rows_kernel_c1_L26_6e_4000.md)"},
         "phases_ms": {"alpha_same_spin_with_diag": parts[0] / args.steps,
                       "beta_same_spin": parts[1] / args.steps, "alpha_beta": ab_ms},
         "flops_per_sigma": alg["flops"], "fp64_tflops": alg["flops"] / (t_step * 1e-3) / 1e12,
