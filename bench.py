@@ -95,6 +95,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings (ms) over all ranks of the
+    process group: the job's time is its slowest rank's."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def measured_peaks():
     try:
         with open(PEAKS_FILE) as f:
@@ -455,9 +464,7 @@ def run_gpu(args):
     t_step = tot / args.steps
     t_e2e = e2e_ms / args.steps
     if pg:
-        tt = torch.tensor([t_step, t_e2e], dtype=torch.float64, device=f"cuda:{dev}")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t_step, t_e2e = tt.tolist()
+        t_step, t_e2e = max_over_ranks([t_step, t_e2e], pg, f"cuda:{dev}")
     if rank != 0:
         ctx.close()
         if pg:

@@ -1,0 +1,64 @@
+"""The N > 1 bookkeeping of bench.py on CPU: two gloo ranks (the GPU path runs
+independent replicas, so its only cross-rank steps are the barrier and the
+max-over-ranks timing), and the reference arm's rule that ranks other than 0
+exit without work."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    assert bench.dist_env() == (rank, world, rank)
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    dist.barrier()
+    # rank r measured (10 + r, 100 - r) ms: the job takes the slowest of each
+    got = bench.max_over_ranks([10.0 + rank, 100.0 - rank], dist, "cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, got))
+
+
+def test_max_over_ranks_gloo_world2():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0] == [11.0, 100.0] and res[1] == [11.0, 100.0]
+
+
+def test_reference_arm_nonzero_rank_exits_without_work(monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    monkeypatch.setenv("LOCAL_RANK", "1")
+
+    class Args:
+        workload = "c2_L36_8e_12000"
+        steps = 1
+        warmup = 0
+        ref_budget = 1.0
+    assert bench.run_reference(Args()) == 0
