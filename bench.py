@@ -392,6 +392,56 @@ def roots_block(args, dev):
             "single_root_seconds": t_one, "single_root_steps": len(te)}
 
 
+def batch_block(args, dev):
+    """args.batch independent problems drawn as the batching workload
+    describes (norb uniform in 10-20, electrons per spin in 3-6, 200-2000
+    selected strings per spin capped at C(norb, ne), seeded integrals per
+    problem): lowest-root FP64 Davidson one problem after another against one
+    sbdgpu_davidson_batch call on the same contexts (set-up done before
+    either), as problems/s, with the largest energy difference."""
+    import math
+    import sbd_b200
+    from sbd_b200 import synth
+    rng = np.random.default_rng(2024)
+    ctxs, sizes = [], []
+    for i in range(args.batch):
+        L = int(rng.integers(10, 21))
+        ne = int(rng.integers(3, 7))
+        cnt = min(int(rng.integers(200, 2001)), math.comb(L, ne))
+        ints, ne, strs = synth.make_small(L, ne, cnt, 1000 + i)
+        c = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+        c.hii()  # tables and diagonal, outside both timings
+        ctxs.append(c)
+        sizes.append(c.n)
+    # the same seeded start for both arms: the aufbau determinant plus a 1 %
+    # random part, so that every run reaches the lowest state whatever its
+    # spin-flip symmetry (from the closed-shell determinant alone, rounding
+    # decides whether a run leaves the spin-flip-even sector)
+    W0s = []
+    for i, c in enumerate(ctxs):
+        w = np.random.default_rng(5000 + i).normal(size=c.n)
+        w *= 0.01 / np.linalg.norm(w)
+        w[0] += 1.0
+        W0s.append(w / np.linalg.norm(w))
+    t = time.perf_counter()
+    e_seq = [c.davidson(w, 100, 10, args.batch_tol)[0] for c, w in zip(ctxs, W0s)]
+    t_seq = time.perf_counter() - t
+    t = time.perf_counter()
+    e_bat, _, steps = sbd_b200.davidson_batch(ctxs, W0s, 100, 10, args.batch_tol)
+    t_bat = time.perf_counter() - t
+    for c in ctxs:
+        c.close()
+    diff = np.abs(np.array(e_bat) - np.array(e_seq))
+    return {"problems": args.batch, "determinants_min": int(min(sizes)), "determinants_max": int(max(sizes)),
+            "determinants_total": int(sum(sizes)), "eps": args.batch_tol,
+            "sequential_problems_per_s": args.batch / t_seq, "batch_problems_per_s": args.batch / t_bat,
+            "speedup": t_seq / t_bat, "max_abs_energy_diff": float(diff.max()),
+            "problems_differing_by_more_than_1e-6": int((diff > 1e-6).sum()),
+            "steps_total": int(sum(steps)), "steps_max": int(max(steps)),
+            "problems_at_step_cap": int(sum(1 for x in steps if x >= 100 * 10)),
+            "note": "one host thread and stream per problem; not a single persistent graph-captured launch"}
+
+
 def run_gpu(args):
     import torch
     import sbd_b200
@@ -516,6 +566,8 @@ def run_gpu(args):
         line["method1_stored"] = method1_block(args, dev, hbm_peak, peak_kind)
     if args.roots > 0:
         line["block_roots"] = roots_block(args, dev)
+    if args.batch > 0:
+        line["batch"] = batch_block(args, dev)
     if not args.no_cpu_baseline:
         try:
             rs = RefSampler(ints, ne, strs)
@@ -547,6 +599,8 @@ def main():
     ap.add_argument("--no-time-to-e0", action="store_true", help="skip the time-to-E0 runs")
     ap.add_argument("--no-method1", action="store_true", help="skip the stored-Hamiltonian (method 1) block")
     ap.add_argument("--roots", type=int, default=0, help="also time block Davidson for this many roots (16M dets)")
+    ap.add_argument("--batch", type=int, default=0, help="also time this many independent small problems at once")
+    ap.add_argument("--batch-tol", type=float, default=1e-6, help="residual target of the batched problems")
     ap.add_argument("--roots-tol", type=float, default=1e-5, help="residual target of the block Davidson block")
     ap.add_argument("--e0-tol", type=float, default=1e-7, help="residual target of the FP64 reference run")
     ap.add_argument("--mixed-tol", type=float, default=1e-3, help="residual target of the mixed runs")

@@ -134,6 +134,16 @@ int sbdgpu_sigma_device_noalloc(sbdgpu_ctx* ctx, const double* dC, double* dsigm
 int sbdgpu_davidson_roots(sbdgpu_ctx* ctx, const sbdgpu_opts* opts, int nroots, double* W, double* energies,
                           double* resid, int* n_iter, int* n_sigma);
 
+/* Lowest-root Davidson (as sbdgpu_davidson, same opts) for nprob independent
+ * problems at once: a pool of max_threads host threads (0: one per problem)
+ * drives the contexts, each on its own stream, so their kernels overlap on the
+ * GPU.  W[i]: problem i's initial vector in, Ritz vector out (reference
+ * convention); energies[i], n_steps[i] (may be NULL) and status[i] (may be
+ * NULL) per problem.  Returns SBDGPU_OK, or the first problem's error status.
+ * The contexts must be distinct and not used by other threads meanwhile. */
+int sbdgpu_davidson_batch(int nprob, sbdgpu_ctx* const* ctxs, const sbdgpu_opts* opts, double* const* W,
+                          double* energies, int* n_steps, int* status, int max_threads);
+
 /* Method 1 (--method 1): build the Hamiltonian's off-diagonal elements once
  * and keep them in device memory, CSR by bra determinant (4-byte ket index and
  * FP64 value per element, 12 bytes); every later FP64 sigma of this context,

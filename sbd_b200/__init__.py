@@ -27,7 +27,7 @@ EXPORTS = [
     "sbdgpu_sigma", "sbdgpu_sigma_device", "sbdgpu_davidson", "sbdgpu_rdm", "sbdgpu_occupation",
     "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
     "sbdgpu_sigma_device_noalloc", "sbdgpu_store_hamiltonian", "sbdgpu_release_hamiltonian",
-    "sbdgpu_davidson_roots", "sbdgpu_wait_selftest",
+    "sbdgpu_davidson_roots", "sbdgpu_wait_selftest", "sbdgpu_davidson_batch",
 ]
 
 
@@ -66,6 +66,9 @@ def lib():
         L.sbdgpu_davidson_roots.argtypes = [_vp, ctypes.POINTER(Opts), ctypes.c_int, _dp, _dp, _dp,
                                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_wait_selftest.argtypes = [_vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_davidson_batch.argtypes = [ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(Opts),
+                                            ctypes.POINTER(_dp), _dp, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.sbdgpu_store_hamiltonian.argtypes = [_vp, _u64p]
         L.sbdgpu_release_hamiltonian.argtypes = [_vp]
         L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
@@ -219,6 +222,26 @@ class Context:
         d = np.zeros(self.na)
         self._check(lib().sbdgpu_alpha_weights(self._h, _p(W, _dp), _p(d, _dp)))
         return d
+
+
+def davidson_batch(ctxs, W0s, max_it: int, max_nb: int, eps: float, precision: int = FP64,
+                   max_time: float = 86400.0, restart_keep: int = 0, restart_prev: int = 0, max_threads: int = 0):
+    """Lowest-root Davidson for several independent contexts at once
+    (sbdgpu_davidson_batch).  Returns (energies, Ritz vectors, steps)."""
+    n = len(ctxs)
+    Ws = [np.ascontiguousarray(w, dtype=np.float64).ravel().copy() for w in W0s]
+    hs = (_vp * n)(*[c._h for c in ctxs])
+    wp = (_dp * n)(*[_p(w, _dp) for w in Ws])
+    o = Opts(max_it, max_nb, eps, max_time, precision, 0, restart_keep, restart_prev)
+    e = np.zeros(n)
+    steps = (ctypes.c_int * n)()
+    st = (ctypes.c_int * n)()
+    rc = lib().sbdgpu_davidson_batch(n, hs, ctypes.byref(o), wp, _p(e, _dp), steps, st, int(max_threads))
+    if rc != 0:
+        bad = [i for i in range(n) if st[i] != 0]
+        msg = lib().sbdgpu_last_error(ctxs[bad[0]]._h) if bad else b""
+        raise SbdGpuError(f"status {rc} (problems {bad}): {msg.decode() if msg else ''}")
+    return e, Ws, [int(x) for x in steps]
 
 
 def context_from_integrals(ints, astr, bstr, device: int = 0) -> Context:

@@ -7,7 +7,10 @@
 #include <cstdio>
 #include <cstring>
 #include <iostream>
+#include <mutex>
 #include <new>
+#include <set>
+#include <utility>
 
 #include "internal.cuh"
 
@@ -24,6 +27,27 @@ void* dev_alloc(size_t bytes) {
                                       cudaGetErrorString(e)};
   }
   return p;
+}
+
+// The dynamic shared-memory limit of a kernel is one attribute per
+// (function, device), shared by every host thread.  Setting it before each
+// launch to that launch's size lets concurrent contexts undercut each other
+// between the set and the launch, which the runtime then rejects.  It is set
+// once instead, to the device's opt-in maximum; each launch still passes its
+// own size.
+void allow_dynamic_smem(const void* func, int device) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({func, device})) return;
+  int optin = 0;
+  SBD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  cudaFuncAttributes fa{};
+  SBD_CUDA(cudaFuncGetAttributes(&fa, func));
+  // dynamic + static shared memory may not pass the opt-in maximum
+  SBD_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)fa.sharedSizeBytes));
+  done.insert({func, device});
 }
 
 void ensure_scratch(sbdgpu_ctx* c) {
@@ -175,12 +199,14 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
     std::vector<float*>* a;
     std::vector<float*>* b;
     double** x;
+    cudaStream_t s;
     ~Free() {
+      cudaStreamSynchronize(s);  // an error path may leave kernels queued on these buffers
       for (auto p : *a) cudaFree(p);
       for (auto p : *b) cudaFree(p);
       cudaFree(*x);
     }
-  } guard{&C, &HC, &X};
+  } guard{&C, &HC, &X, st};
   for (int k = 0; k < nb; k++) {
     C[k] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
     HC[k] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
@@ -203,11 +229,13 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
   struct FreeT {
     std::vector<float*>* a;
     std::vector<float*>* b;
+    cudaStream_t s;
     ~FreeT() {
+      cudaStreamSynchronize(s);
       for (auto p : *a) cudaFree(p);
       for (auto p : *b) cudaFree(p);
     }
-  } guard_t{&T, &TH};
+  } guard_t{&T, &TH, st};
   if (keep > 1)
     for (int j = 0; j < keep; j++) {
       T[j] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
@@ -519,13 +547,15 @@ int sbdgpu_davidson(sbdgpu_ctx* c, const sbdgpu_opts* o, double* Wh, double* ene
       std::vector<double*>* b;
       double** w;
       double** r;
+      cudaStream_t s;
       ~Free() {
+        cudaStreamSynchronize(s);  // an error path may leave kernels queued on these buffers
         for (auto p : *a) cudaFree(p);
         for (auto p : *b) cudaFree(p);
         cudaFree(*w);
         cudaFree(*r);
       }
-    } guard{&C, &HC, &W, &R};
+    } guard{&C, &HC, &W, &R, st};
     W = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
     R = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
     SBD_CUDA(cudaMemcpyAsync(W, Wh, sizeof(double) * n, cudaMemcpyHostToDevice, st));

@@ -168,5 +168,6 @@ void ensure_scratch(sbdgpu_ctx* c);
 void ensure_io(sbdgpu_ctx* c);
 void jacobi_eig(int n, double* A, int lda, double* w);
 void* dev_alloc(size_t bytes);
+void allow_dynamic_smem(const void* func, int device);
 
 }  // namespace sbdgpu

@@ -48,12 +48,14 @@ void davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, double* Wh,
   struct Free {
     std::vector<double*>* v[4];
     double** x[2];
+    cudaStream_t s;
     ~Free() {
+      cudaStreamSynchronize(s);  // an error path may leave kernels queued on these buffers
       for (auto* a : v)
         for (auto p : *a) cudaFree(p);
       for (auto* p : x) cudaFree(*p);
     }
-  } guard{{&C, &HC, &T, &TH}, {&X, &R}};
+  } guard{{&C, &HC, &T, &TH}, {&X, &R}, st};
   for (int k = 0; k < max_sub; k++) {
     C[k] = (double*)dev_alloc(sizeof(double) * n);
     HC[k] = (double*)dev_alloc(sizeof(double) * n);

@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(NT) ab_kernel(
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (size_t sl = warp; sl < nslice; sl += nwarp) {
     size_t ib = sl * 32 + lane;
+    if (ib >= nb) continue;  // padding lane of the last slice (no warp-wide operation below)
     int w = sell_w[sl];
     const uint32_t* ent = sell + sell_off[sl] + lane;
     T y[G];
@@ -298,11 +299,11 @@ void launch_ab(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem) {
   dim3 grid((unsigned)c->na, (unsigned)((ta.max_s + G - 1) / G));
   if (grid.y == 0) return;
   if (2 * (smem + 1024) <= 228 * 1024) {
-    SBD_CUDA(cudaFuncSetAttribute(ab_kernel<T, G, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<T, G, 512>), c->device);
     ab_kernel<T, G, 512><<<grid, 512, smem, c->stream>>>(C, S, c->nb, c->P, vf, ta.s_off, ta.s_idx, ta.s_info,
                                                          tb.sell_off, tb.sell_w, tb.sell, tb.nslice);
   } else {
-    SBD_CUDA(cudaFuncSetAttribute(ab_kernel<T, G, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<T, G, 1024>), c->device);
     ab_kernel<T, G, 1024><<<grid, 1024, smem, c->stream>>>(C, S, c->nb, c->P, vf, ta.s_off, ta.s_idx, ta.s_info,
                                                            tb.sell_off, tb.sell_w, tb.sell, tb.nslice);
   }

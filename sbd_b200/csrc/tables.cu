@@ -109,12 +109,15 @@ __global__ void fill_kernel(const uint64_t* __restrict__ s, int n, int L, const 
 __global__ void sell_fill_kernel(int n, const int64_t* __restrict__ s_off, const int32_t* __restrict__ s_idx,
                                  const uint32_t* __restrict__ s_info, const int64_t* __restrict__ sell_off,
                                  const int32_t* __restrict__ sell_w, uint32_t* sell) {
+  // every lane of every slice, the padding lanes past the last bra string
+  // included: those get kSellInvalid entries, never uninitialised memory
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  int nslice = (n + kSlice - 1) / kSlice;
+  if (i >= nslice * kSlice) return;
   int slice = i / kSlice, lane = i % kSlice;
   int64_t base = sell_off[slice];
   int w = sell_w[slice];
-  int64_t b = s_off[i], e = s_off[i + 1];
+  int64_t b = i < n ? s_off[i] : 0, e = i < n ? s_off[i + 1] : 0;
   for (int t = 0; t < w; t++) {
     uint32_t v = kSellInvalid;
     if (b + t < e) {
@@ -184,8 +187,9 @@ static void build_one(sbdgpu_ctx* c, SpinTables& t, const uint64_t* dstr, size_t
   SBD_CUDA(cudaMemcpyAsync(t.sell_off, so.data(), sizeof(int64_t) * (t.nslice + 1), cudaMemcpyHostToDevice, st));
   SBD_CUDA(cudaMemcpyAsync(t.sell_w, w.data(), sizeof(int32_t) * t.nslice, cudaMemcpyHostToDevice, st));
   if (n) {
-    sell_fill_kernel<<<(ni + 255) / 256, 256, 0, st>>>(ni, t.s_off, t.s_idx, t.s_info, t.sell_off, t.sell_w,
-                                                      t.sell);
+    const int nlanes = (int)(t.nslice * kSlice);
+    sell_fill_kernel<<<(nlanes + 255) / 256, 256, 0, st>>>(ni, t.s_off, t.s_idx, t.s_info, t.sell_off, t.sell_w,
+                                                          t.sell);
     SBD_CUDA(cudaGetLastError());
   }
   SBD_CUDA(cudaStreamSynchronize(st));

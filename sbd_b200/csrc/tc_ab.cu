@@ -427,7 +427,7 @@ void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
   a.P = c->P;
   a.mtiles = (c->P + 127) / 128;
   size_t smem = tc_smem_bytes(a.mtiles, c->na);
-  SBD_CUDA(cudaFuncSetAttribute(tc_ab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(reinterpret_cast<const void*>(tc_ab_kernel), c->device);
   int sms = 148;
   SBD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   int grid = (int)std::min<size_t>((size_t)sms, c->nb);

@@ -212,3 +212,22 @@ def test_rdm_energy_equals_sigma_expectation(case):
     ne_a = bin(int(a[0])).count("1")
     ne_b = bin(int(b[0])).count("1")
     assert abs(np.trace(o[0]) - ne_a) < 1e-10 and abs(np.trace(o[1]) - ne_b) < 1e-10
+
+
+def test_sigma_after_dirty_device_memory():
+    """Sliced-ELL padding lanes past the last beta string are written, not
+    left as whatever the allocation held: fill device memory with 0xFF bytes,
+    release it to the driver, then build tables and sigma for a basis whose
+    string counts are not multiples of 32, against the oracle."""
+    import torch
+    buf = torch.full((1 << 28,), 255, dtype=torch.uint8, device="cuda:0")
+    torch.cuda.synchronize()
+    del buf
+    torch.cuda.empty_cache()
+    ints, a, b = _seeded_system(10, 3, 45, 13, ragged=True)
+    assert len(a) % 32 and len(b) % 32
+    ctx = sbd_b200.context_from_integrals(ints, a, b)
+    orc = oracle.Oracle(10, a, b, ints.ecore, ints.h, ints.eri)
+    C = seeded_vector(ctx.n, 13)
+    ref = orc.sigma(C)
+    assert np.abs(ctx.sigma(C) - ref).max() <= 1e-12 * np.abs(ref).max()
