@@ -17,7 +17,8 @@
  * The run is MPI world size 1 on one GPU: the communicator argument is
  * accepted for signature compatibility; with a real MPI build a communicator
  * of more than one rank is rejected.  Added options (not in the reference):
- * SBD::device (--device), SBD::precision (--precision).
+ * SBD::device (--device), SBD::precision (--precision), SBD::restart_keep
+ * (--restart_keep) and SBD::restart_prev (--restart_prev).
  */
 #ifndef SBD_GPU_TPB_H
 #define SBD_GPU_TPB_H
@@ -366,6 +367,8 @@ struct SBD {
   size_t bit_length = 20;
   int device = 0;     // added: CUDA device
   int precision = 0;  // added: SBDGPU_FP64
+  int restart_keep = 0;  // added: mixed precisions, Ritz vectors kept at a restart (0/1: collapse)
+  int restart_prev = 0;  // added: mixed precisions, also keep the previous Ritz vector
 };
 
 inline SBD generate_sbd_data(int argc, char* argv[]) {
@@ -388,6 +391,8 @@ inline SBD generate_sbd_data(int argc, char* argv[]) {
     else if (a == "--bit_length") d.bit_length = (size_t)std::atoi(v);
     else if (a == "--device") d.device = std::atoi(v);
     else if (a == "--precision") d.precision = std::atoi(v);
+    else if (a == "--restart_keep") d.restart_keep = std::atoi(v);
+    else if (a == "--restart_prev") d.restart_prev = std::atoi(v);
     else hit = false;
     if (hit) i++;
   }
@@ -458,7 +463,8 @@ inline void diag(const MPI_Comm& comm, const SBD& sbd_data, const FCIDump& fcidu
     std::cout << " method " << sbd_data.method
               << ": the GPU path builds H*C on the fly (method 0); results are the same" << std::endl;
   }
-  sbdgpu_opts o{sbd_data.max_it, sbd_data.max_nb, sbd_data.eps, sbd_data.max_time, sbd_data.precision, 1, 0, 0};
+  sbdgpu_opts o{sbd_data.max_it,    sbd_data.max_nb, sbd_data.eps,          sbd_data.max_time,
+                sbd_data.precision, 1,               sbd_data.restart_keep, sbd_data.restart_prev};
   double e = 0.0;
   int steps = 0;
   auto t_dav = std::chrono::high_resolution_clock::now();

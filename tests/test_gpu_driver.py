@@ -51,3 +51,19 @@ def test_sample_driver_matches_reference():
         e2 = float(re.search(r"Sample-based diagonalization: Energy = (\S+)", r2.stdout).group(1))
         assert abs(e2 - float(g["energy"])) < 1e-10
         assert r2.stdout.count("Davidson iteration") == 1
+
+
+def test_sample_driver_mixed_with_restarts():
+    """The added options reach the solver: FP32 basis with thick restart and
+    the previous Ritz vector gives the reference's energy to 1e-6 Eh."""
+    g = load_golden("g_L8_3e_full")
+    exe = build.build_driver()
+    ints, ne, strs = synth.make_small(8, 3, None, int(g["seed"]))
+    with tempfile.TemporaryDirectory() as td:
+        fp, dp = synth.write_workload(td, ints, ne, strs)
+        r = subprocess.run([exe, "--fcidump", fp, "--adetfile", dp, "--block", "10", "--iteration", "1000",
+                            "--tolerance", "1e-5", "--rdm", "0", "--precision", "1", "--restart_keep", "3",
+                            "--restart_prev", "1"], cwd=td, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        e = float(re.search(r"Sample-based diagonalization: Energy = (\S+)", r.stdout).group(1))
+        assert abs(e - float(g["energy"])) < 1e-6
