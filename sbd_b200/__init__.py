@@ -237,6 +237,8 @@ def davidson_batch(ctxs, W0s, max_it: int, max_nb: int, eps: float, precision: i
     steps = (ctypes.c_int * n)()
     st = (ctypes.c_int * n)()
     rc = lib().sbdgpu_davidson_batch(n, hs, ctypes.byref(o), wp, _p(e, _dp), steps, st, int(max_threads))
+    if rc == 1 and all(st[i] == 0 for i in range(n)):
+        raise SbdGpuError("status 1: invalid arguments (null pointers or a context given twice)")
     if rc != 0:
         bad = [i for i in range(n) if st[i] != 0]
         msg = lib().sbdgpu_last_error(ctxs[bad[0]]._h) if bad else b""

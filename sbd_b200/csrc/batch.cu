@@ -19,6 +19,12 @@ extern "C" int sbdgpu_davidson_batch(int nprob, sbdgpu_ctx* const* ctxs, const s
   if (nprob < 0 || (nprob > 0 && (!ctxs || !opts || !W || !energies))) return SBDGPU_ERR_ARG;
   for (int i = 0; i < nprob; i++)
     if (!ctxs[i] || !W[i]) return SBDGPU_ERR_ARG;
+  {
+    // one thread per context at a time: the same context twice would race
+    std::vector<sbdgpu_ctx*> seen(ctxs, ctxs + nprob);
+    std::sort(seen.begin(), seen.end());
+    if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) return SBDGPU_ERR_ARG;
+  }
   int nt = max_threads > 0 ? std::min(max_threads, nprob) : nprob;
   std::atomic<int> next{0};
   std::vector<int> st(nprob, SBDGPU_OK);

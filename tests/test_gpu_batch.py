@@ -41,3 +41,10 @@ def test_batch_matches_single_runs(threads):
         assert abs(abs(np.dot(w, w1)) - 1.0) < 1e-8
     assert abs(E[-1] - float(g["energy"])) < 1e-10
     assert all(s > 0 for s in steps)
+
+
+def test_batch_rejects_a_context_given_twice():
+    g = load_golden("g_L8_3e_full")
+    c = gpu_ctx(g)
+    with pytest.raises(sbd_b200.SbdGpuError, match="twice"):
+        sbd_b200.davidson_batch([c, c], [_unit(c.n), _unit(c.n)], 10, 10, 1e-6)
