@@ -62,3 +62,24 @@ def test_reference_arm_nonzero_rank_exits_without_work(monkeypatch):
         warmup = 0
         ref_budget = 1.0
     assert bench.run_reference(Args()) == 0
+
+
+def test_reference_arm_json_contract():
+    """bench.py --impl reference on rank 0 (CPU only): one JSON line with the
+    contract's keys, timing the compiled reference's own mult."""
+    import json
+    import subprocess
+    import oracle
+    if not oracle.reference_available():
+        pytest.skip("compiled reference not available")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--workload", "c1_L26_6e_4000", "--ref-budget", "5"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=600,
+                       env={**os.environ, "RANK": "0", "WORLD_SIZE": "1"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
+    for k in ("metric", "unit", "config", "cpu_baseline", "e2e", "steps", "warmup"):
+        assert k in line
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
