@@ -110,6 +110,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// One bucket entry: goff | neg<<14 | ia<<15, goff = row * kGStride + column of
+// the staged tile.  sigma[ia] += (-1)^neg G[goff], the sign applied by
+// flipping the float's sign bit.
+__device__ __forceinline__ void tc_scatter(const float* G, float* sig, uint32_t en) {
+  const uint32_t g = __float_as_uint(G[en & 0x3FFFu]) ^ ((en << 17) & 0x80000000u);
+  atomicAdd(&sig[en >> 15], __uint_as_float(g));
+}
+
 struct TcArgs {
   const __nv_bfloat16* ct16;  // C^T in BF16, [nb][na_pad] (zero padded), alpha-string-major convention
   float* out;            // [nb][na] alpha-beta part of sigma, transposed
@@ -118,7 +126,7 @@ struct TcArgs {
   const int32_t* b_idx;
   const uint32_t* b_info;
   const int64_t* bk_off;   // alpha-pair buckets by (ja tile, M tile)
-  const uint32_t* bk_ent;  // ja_local | pq_local<<6 | neg<<13 | ia<<14
+  const uint32_t* bk_ent;  // (pq_local * kGStride + ja_local) | neg<<14 | ia<<15
   int* err;
   int na, nb, P, mtiles, na_pad;
 };
@@ -276,18 +284,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
 #pragma unroll
           for (int u = 0; u < kEntPerMt; u++) {
             const uint32_t en = ent[mt][u];
-            if (en != 0xFFFFFFFFu) {
-              const int jl = en & 63u, pl = (en >> 6) & 127u, ia = (int)(en >> 14);
-              const float g = G[pl * kGStride + jl];
-              atomicAdd(&sig[ia], (en & (1u << 13)) ? -g : g);
-            }
+            if (en != 0xFFFFFFFFu) tc_scatter(G, sig, en);
           }
           // entries beyond the prefetched ones
           for (int64_t e = s_bo[mt] + tid + (int64_t)kEntPerMt * kTcThreads; e < s_bo[mt + 1]; e += kTcThreads) {
-            const uint32_t en = __ldg(&a.bk_ent[e]);
-            const int jl = en & 63u, pl = (en >> 6) & 127u, ia = (int)(en >> 14);
-            const float g = G[pl * kGStride + jl];
-            atomicAdd(&sig[ia], (en & (1u << 13)) ? -g : g);
+            tc_scatter(G, sig, __ldg(&a.bk_ent[e]));
           }
           __syncthreads();
         }
@@ -359,8 +360,9 @@ void wait_selftest(sbdgpu_ctx* c, long long limit, int* status) {
 
 bool tc_ab_supported(const sbdgpu_ctx* c) {
   int mtiles = (c->P + 127) / 128;
-  // na < 2^18: an entry of all ones (ia = 2^18 - 1) is the empty-register marker
-  return mtiles <= kTcMaxMTiles && c->na < (1 << 18) && tc_smem_bytes(mtiles, c->na) <= 225 * 1024;
+  // na < 2^17: ia takes bits 15..31 of an entry, and an entry of all ones is
+  // the empty-register marker
+  return mtiles <= kTcMaxMTiles && c->na < (1 << 17) - 1 && tc_smem_bytes(mtiles, c->na) <= 225 * 1024;
 }
 
 // Alpha singles bucketed by (tile of 64 source strings ja, M tile of 128 pq).
@@ -384,7 +386,8 @@ void build_tc_buckets(sbdgpu_ctx* c) {
       uint32_t neg = (info[k] >> 31) & 1u;
       uint32_t ia = (uint32_t)idx[k];
       size_t tile = ja / kTcN;
-      uint32_t e = (uint32_t)(ja % kTcN) | ((pq % 128u) << 6) | (neg << 13) | (ia << 14);
+      uint32_t goff = (pq % 128u) * (uint32_t)kGStride + (uint32_t)(ja % kTcN);  // < 2^14
+      uint32_t e = goff | (neg << 14) | (ia << 15);
       bucket[tile * mtiles + pq / 128].push_back(e);
     }
   }
