@@ -18,7 +18,8 @@ def pytest_configure(config):
 def _ensure_built():
     import oracle
     from sbd_b200 import build
-    if not os.path.exists(oracle.ORACLE_SO) or (os.path.exists("/root/reference") and not os.path.exists(oracle.REF_SO)):
+    # make builds the reference checker only where the reference checkout is present
+    if not os.path.exists(oracle.ORACLE_SO) or not oracle.reference_available():
         oracle.build()
     if not os.path.exists(build.LIB):
         build.build_lib()
