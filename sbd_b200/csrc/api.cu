@@ -179,6 +179,10 @@ void sigma_ref_convention(sbdgpu_ctx* c, const double* dC, double* dS, int preci
 // Gram-Schmidt; the energy is the FP64 Rayleigh quotient <W|H W> from one FP64
 // refinement sigma of the final Ritz vector (the same final step as
 // chemistry/tpb/sbdiag.h:239-262).  Vectors in the alpha-string-major convention.
+// Restarts: the reference's collapse to W, or (restart_keep > 1) the lowest
+// Ritz vectors with their sigma vectors, optionally (restart_prev) with the
+// previous step's Ritz vector as well; with vectors carried over, the
+// correction is orthogonalised in two Gram-Schmidt passes.
 void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, double* energy, double* trace_e,
                     double* trace_tol, int max_trace, int* n_steps) {
   // SBDGPU_MIXED_TC: tensor-core sigma while the residual norm is above this,

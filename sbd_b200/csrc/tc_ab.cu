@@ -7,18 +7,22 @@
 // For one beta string ib the second line is a dense GEMM: M = folded alpha
 // pair index pq (P = L(L+1)/2 rows, tiles of 128), N = source alpha string ja
 // (tiles of 64), K = the beta singles of ib (chunks of 80).  One CTA owns one
-// ib at a time (persistent over ib), keeps the A operand (pq|rs_t) for the
-// current K chunk in shared memory, streams B = sb_t C[ja, jb_t] tiles from
-// the transposed vector, and issues tcgen05.mma from one thread into TMEM
-// (one 128 x 64 FP32 accumulator per M tile).  The epilogue reads TMEM
-// (tcgen05.ld), stages one M tile in shared memory and adds the entries that
-// are real alpha singles into the CTA's FP32 sigma column with shared-memory
-// atomics; the column is written once per ib into a [nb][na] buffer.
+// ib at a time (persistent over ib), keeps the A operand sb_t (pq|rs_t) for
+// the current K chunk in shared memory, streams B = C[ja, jb_t] tiles from the
+// BF16 transposed vector with cp.async (double buffered), and issues
+// tcgen05.mma from one thread into TMEM (one 128 x 64 FP32 accumulator per M
+// tile).  The epilogue (16 warps, each reading one 32-lane x 16-column block
+// of TMEM with tcgen05.ld) stages one M tile in shared memory and adds the
+// entries that are real alpha singles, prefetched into registers while the
+// MMAs ran, into the CTA's FP32 sigma column with shared-memory atomics; the
+// column is written once per ib into a [nb][na] buffer.
 //
-// Operands use the canonical K-major layout without swizzle: 8-row x 16-byte
-// core matrices, LBO = 128 B between core matrices along K, SBO = 10 x 128 B
-// between 8-row groups.  Every wait on the MMA completion barrier is bounded;
-// on timeout the kernel records an error, frees its tensor memory and returns.
+// Layouts without swizzle: A is K-major (8-row x 16-byte core matrices,
+// LBO = 128 B between core matrices along K, SBO = 10 x 128 B between 8-row
+// groups); B is MN-major (core matrix = 8 K rows x 8 consecutive ja), so each
+// 16-byte chunk is one cp.async from a row of the transposed vector.  Every
+// wait on the MMA completion barrier is bounded; on timeout the kernel records
+// an error, frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
