@@ -113,31 +113,14 @@ def measured_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic_per_det():
-    """DRAM bytes per determinant of one alpha-beta kernel launch, from the
-    committed ncu summary (captured on a smaller workload, scaled by the
-    determinant count)."""
-    p = os.path.join(ROOT, "profiles", "ab_kernel_c1_L26_6e_4000.md")
-    try:
-        for line in open(p):
-            if line.startswith("traffic_bytes_per_determinant:"):
-                return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
-
-
-def profiled_spmv_traffic():
-    """DRAM bytes of one stored-Hamiltonian product launch at the
-    245,025-determinant case, from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "spmv_kernel_c0_L12_4e_full.md")
-    try:
-        for line in open(p):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one launch,
+# from single captures of smaller workloads of the same kernels:
+#  - ab_kernel<double> at 16M determinants (norb 26, 6a/6b, 4000 strings):
+#    1192.4 MB per launch, 74.5 bytes per determinant; the 144M line scales it
+#    by the determinant count
+#  - spmv_kernel (method 1) at 245,025 determinants: 4.236 GB per launch
+AB_TRAFFIC_BYTES_PER_DET = 74.5
+SPMV_TRAFFIC_BYTES_C0 = 4.236e9
 
 
 def table_stats(ctx):
@@ -250,7 +233,10 @@ def run_reference(args):
             break
     rs.close()
     v = len(vals) / sum(1.0 / x for x in vals)  # total elements / total time
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+    # steps = samples actually timed (the run stops adding samples after
+    # --ref-budget seconds); no warm-up sample is taken
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": len(vals), "warmup": 0,
+            "steps_requested": args.steps, "ref_budget_s": args.ref_budget, "sampled_seconds": spent,
             "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded integrals and strings)", "impl": "reference",
             "config": {"workload": args.workload, "determinants": int(len(strs)) ** 2, "norb": ints.norb,
@@ -362,7 +348,7 @@ def method1_block(args, dev, hbm_peak, peak_kind):
             "sigma_per_s": 1000.0 * len(tot) / sum(tot), "on_the_fly_sigma_per_s": 1000.0 * len(fly) / sum(fly),
             "roofline": {"bound": "hbm", "kernel": "spmv_kernel (stored Hamiltonian)", "achieved": achieved,
                          "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_kind,
-                         "algorithmic_bytes": bytes_per, "traffic": profiled_spmv_traffic()},
+                         "algorithmic_bytes": bytes_per, "traffic": SPMV_TRAFFIC_BYTES_C0},
             "note": "12 bytes per stored element (uint32 ket, FP64 value) + row offsets + hii, C, sigma"}
 
 
@@ -531,8 +517,7 @@ def run_gpu(args):
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     traffic = args.traffic
     if traffic is None and dom == 2:
-        tpd = profiled_traffic_per_det()
-        traffic = tpd * n if tpd else None
+        traffic = AB_TRAFFIC_BYTES_PER_DET * n
     line = {
         "metric": METRIC, "value": world * 1000.0 / t_step, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",

@@ -110,12 +110,14 @@ int sbdgpu_sigma_device(sbdgpu_ctx* ctx, const double* dC, double* dsigma, int p
  * device, or the call sits on a path that must not synchronise the device as
  * cudaMalloc/cudaFree can).  No counterpart in the reference.  It allocates
  * nothing: its scratch is one 12 MiB file-scope device array (3 x 524,288
- * doubles) that every GPU loading this library holds until exit.  Limits:
+ * doubles) that every GPU with a context holds until exit.  Limits:
  * na*nb <= 524,288 (SBDGPU_ERR_LIMIT otherwise); the context's set-up must be
- * done first (sbdgpu_build_tables and sbdgpu_diag, else SBDGPU_ERR_STATE); the
- * first call on a device resolves the array's address and should come before
- * any stream capture; all calls share the array, so calls that overlap on the
- * GPU race.  Same result as sbdgpu_sigma_device, FP64 only. */
+ * done first (sbdgpu_build_tables and sbdgpu_diag, else SBDGPU_ERR_STATE).
+ * sbdgpu_create resolves the array's address on its device and loads the
+ * sigma kernels there, so the call itself loads no module (CUDA's lazy
+ * loading would otherwise allocate inside it).  All calls share the array, so
+ * calls that overlap on the GPU race.  Same result as sbdgpu_sigma_device,
+ * FP64 only. */
 int sbdgpu_sigma_device_noalloc(sbdgpu_ctx* ctx, const double* dC, double* dsigma);
 
 /* Block Davidson for the nroots lowest roots, FP64 (an extension: the
@@ -135,7 +137,8 @@ int sbdgpu_davidson_roots(sbdgpu_ctx* ctx, const sbdgpu_opts* opts, int nroots, 
                           double* resid, int* n_iter, int* n_sigma);
 
 /* Lowest-root Davidson (as sbdgpu_davidson, same opts) for nprob independent
- * problems at once: a pool of max_threads host threads (0: one per problem)
+ * problems at once: a pool of max_threads host threads (0: one per problem,
+ * capped at the host's hardware threads and at 32)
  * drives the contexts, each on its own stream, so their kernels overlap on the
  * GPU.  W[i]: problem i's initial vector in, Ritz vector out (reference
  * convention); energies[i], n_steps[i] (may be NULL) and status[i] (may be
@@ -199,7 +202,8 @@ int sbdgpu_last_sigma_ms(sbdgpu_ctx* ctx, float* ms5);
  * waits on a barrier nobody arrives on, polling at most spin_limit times, and
  * one that arrives first.  status[0] = 1 when the first wait gave up (the
  * expected outcome), status[1] = 0 when the second completed.  The context
- * stays usable either way. */
+ * stays usable either way.  spin_limit in [1, 2^26] (the kernel's own limit),
+ * else SBDGPU_ERR_ARG; each wait also gives up after 2 s of GPU time. */
 int sbdgpu_wait_selftest(sbdgpu_ctx* ctx, long long spin_limit, int* status);
 
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);

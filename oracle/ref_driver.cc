@@ -18,7 +18,7 @@
  *   sbdref_diag        sbd::tpb::diag (chemistry/tpb/sbdiag.h:102-456)
  *   sbdref_correlation Correlation (chemistry/tpb/correlation.h:194-443)
  *   sbdref_occupation  OccupationDensity (chemistry/tpb/occupation.h:10-95)
- *   sbdref_carryover   CarryOverAlphaDet (chemistry/tpb/rdmat.h:159-231)
+ *   sbdref_carryover   CarryOverAlphaDet (chemistry/tpb/rdmat.h:60-132)
  *   sbdref_save_wavefunction / sbdref_load_wavefunction
  *                      SaveWavefunction / LoadWavefunction (chemistry/tpb/restart.h:20-66,
  *                      414-658), the load mapping a saved basis onto this handle's

@@ -429,6 +429,8 @@ int sbdgpu_create(sbdgpu_ctx** out, int norb, size_t na, size_t nb, const uint64
     SBD_CUDA(cudaMemcpyAsync(c->h1, h1, sizeof(double) * norb * norb, cudaMemcpyHostToDevice, c->stream));
     SBD_CUDA(cudaMemcpyAsync(c->vf, c->h_vf.data(), sizeof(double) * P * P, cudaMemcpyHostToDevice, c->stream));
     SBD_CUDA(cudaStreamSynchronize(c->stream));
+    // once per device: the no-allocation sigma's scratch address and kernels
+    sbdgpu::noalloc_prepare(device);
   });
   if (rc != SBDGPU_OK) {
     std::fprintf(stderr, "sbdgpu_create: %s\n", c->err.c_str());
@@ -655,7 +657,8 @@ int sbdgpu_davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, doubl
 
 int sbdgpu_wait_selftest(sbdgpu_ctx* c, long long spin_limit, int* status) {
   return guarded(c, [&] {
-    if (!status || spin_limit < 1) throw Error{SBDGPU_ERR_ARG, "status must be non-null and spin_limit >= 1"};
+    if (!status || spin_limit < 1 || spin_limit > sbdgpu::kMaxSpinLimit)
+      throw Error{SBDGPU_ERR_ARG, "status must be non-null and spin_limit in [1, 2^26]"};
     sbdgpu::wait_selftest(c, spin_limit, status);
   });
 }

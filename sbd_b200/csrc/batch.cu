@@ -25,7 +25,10 @@ extern "C" int sbdgpu_davidson_batch(int nprob, sbdgpu_ctx* const* ctxs, const s
     std::sort(seen.begin(), seen.end());
     if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) return SBDGPU_ERR_ARG;
   }
-  int nt = max_threads > 0 ? std::min(max_threads, nprob) : nprob;
+  // default pool: one thread per problem, at most one per host hardware
+  // thread and at most 32 (each thread drives its own stream)
+  const int hw = std::max(1, (int)std::thread::hardware_concurrency());
+  int nt = max_threads > 0 ? std::min(max_threads, nprob) : std::min({nprob, hw, 32});
   std::atomic<int> next{0};
   std::vector<int> st(nprob, SBDGPU_OK);
   auto work = [&] {

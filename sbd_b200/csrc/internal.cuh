@@ -39,6 +39,9 @@ struct Error {
   } while (0)
 
 constexpr uint32_t kSellInvalid = 0xFFFFFFFFu;
+// polls of a bounded mbarrier wait (the tensor-core kernel's, and the largest
+// limit sbdgpu_wait_selftest accepts)
+constexpr long long kMaxSpinLimit = 1ll << 26;
 constexpr int kSlice = 32;
 
 struct SpinTables {
@@ -158,10 +161,15 @@ void davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, double* Wh,
                     int* n_iter, int* n_sigma);
 
 // sigma.cu
+void preload_fp64_sigma(int device);
+void preload_fp64_sigma_misc();  // misc.cu
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);
 void sigma_fp64_prepared(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st);
 void sigma_fp32(sbdgpu_ctx* c, const float* C, float* S);
 void sigma_fp32_tc(sbdgpu_ctx* c, const float* C, float* S);
+
+// noalloc.cu
+void noalloc_prepare(int device);
 
 // api.cu
 void ensure_scratch(sbdgpu_ctx* c);

@@ -470,6 +470,16 @@ void transpose_add(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s
   SBD_CUDA(cudaGetLastError());
 }
 
+// Loads this file's kernels of the FP64 sigma path (sign phase, transposes)
+// on the current device now rather than at their first launch: with CUDA's
+// lazy module loading, a first launch loads the module and may allocate.
+void preload_fp64_sigma_misc() {
+  cudaFuncAttributes fa{};
+  SBD_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(phase_kernel)));
+  SBD_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(transpose_kernel<double, false>)));
+  SBD_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(transpose_kernel<double, true>)));
+}
+
 template void transpose<double>(const double*, double*, size_t, size_t, cudaStream_t);
 template void transpose<float>(const float*, float*, size_t, size_t, cudaStream_t);
 template void transpose_add<double>(const double*, double*, size_t, size_t, cudaStream_t);

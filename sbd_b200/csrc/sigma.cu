@@ -345,7 +345,30 @@ void sigma_launch(sbdgpu_ctx* c, const T* C, T* S, T* ct, T* st, const T* ja, co
   if (events) SBD_CUDA(cudaEventRecord(c->ev[3], s));
 }
 
+template <int G>
+void preload_ab(int device) {
+  allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<double, G, 512>), device);
+  allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<double, G, 1024>), device);
+}
+
 }  // namespace
+
+// Loads every kernel that an FP64 sigma build can launch on the current
+// device now (and sets the alpha-beta kernels' shared-memory limit), instead
+// of at first launch, where CUDA's lazy module loading may allocate.
+void preload_fp64_sigma(int device) {
+  cudaFuncAttributes fa{};
+  SBD_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(rows_kernel<double, true>)));
+  SBD_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(rows_kernel<double, false>)));
+  SBD_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(rows_vec_kernel<double, true>)));
+  SBD_CUDA(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(rows_vec_kernel<double, false>)));
+  preload_ab<16>(device);
+  preload_ab<8>(device);
+  preload_ab<4>(device);
+  preload_ab<2>(device);
+  preload_ab<1>(device);
+  preload_fp64_sigma_misc();
+}
 
 void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S) {
   build_tables(c);

@@ -47,7 +47,8 @@ constexpr int kTcMaxMTiles = 8;                 // 8 x 64 = 512 TMEM columns
 constexpr int kWarpCols = kTcN * 4 / (kTcThreads / 32);  // accumulator columns per warp in the epilogue
 static_assert(kWarpCols % 16 == 0 && kWarpCols >= 16, "epilogue reads 16-column groups");
 constexpr int kGStride = kTcN + 4;  // epilogue staging row: 16-byte stores of 8 lanes hit distinct banks
-constexpr long long kSpinLimit = 1ll << 26;
+constexpr long long kSpinLimit = kMaxSpinLimit;
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: an MMA tile completes in microseconds
 constexpr int kEntPerMt = 2;  // bucket entries per thread and M tile prefetched into registers
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -89,7 +90,18 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit = kSpinLimit) {
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Polls the barrier at most `limit` times and for at most `max_ns`
+// nanoseconds of the global timer (checked every 1024 polls), whichever ends
+// first; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit = kSpinLimit,
+                                          uint64_t max_ns = kWaitNs) {
+  const uint64_t t0 = global_ns();
   for (long long i = 0; i < limit; i++) {
     uint32_t done;
     asm volatile(
@@ -99,6 +111,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long l
         : "r"(mbar), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((i & 1023) == 1023 && global_ns() - t0 > max_ns) return false;
   }
   return false;
 }
@@ -442,10 +455,13 @@ void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
   SBD_CUDA(cudaGetLastError());
 }
 
+// Reads and clears the timeout flag: a timeout is reported once, and the
+// context's later tensor-core sigma builds start clean.
 int tc_error(sbdgpu_ctx* c) {
   if (!c->tc_err) return 0;
   int h = 0;
   SBD_CUDA(cudaMemcpyAsync(&h, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SBD_CUDA(cudaMemsetAsync(c->tc_err, 0, sizeof(int), c->stream));
   SBD_CUDA(cudaStreamSynchronize(c->stream));
   return h;
 }

@@ -12,7 +12,7 @@
  *   DecodeAlphaDets, ShuffleDet          makedeterminants.h:63-108, determinants.h:566-571
  *   sbd::tpb::SBD, generate_sbd_data     chemistry/tpb/sbdiag.h:12-85
  *   SaveWavefunction, LoadWavefunction   chemistry/tpb/restart.h:20-66, 414-658
- *   CarryOverAlphaDet (both variants)    chemistry/tpb/rdmat.h:159-231
+ *   CarryOverAlphaDet (both variants)    chemistry/tpb/rdmat.h:60-132
  *   sbd::tpb::diag (both overloads)      chemistry/tpb/sbdiag.h:102-565
  * The run is MPI world size 1 on one GPU: the communicator argument is
  * accepted for signature compatibility; with a real MPI build a communicator
@@ -311,7 +311,7 @@ void LoadWavefunction(const std::string& file, const std::vector<std::vector<siz
   for (auto& x : W) x /= nrm;
 }
 
-// rdmat.h:159-196 (cumulative-weight threshold)
+// rdmat.h:60-97 (cumulative-weight threshold)
 inline void CarryOverAlphaDet(const std::vector<double>& D, const std::vector<std::vector<size_t>>& adet,
                               std::vector<std::vector<size_t>>& rdet, double threshold) {
   size_t n = adet.size();
@@ -330,7 +330,7 @@ inline void CarryOverAlphaDet(const std::vector<double>& D, const std::vector<st
   for (size_t k = 0; k < imax; k++) rdet[k] = adet[idx[k]];
 }
 
-// rdmat.h:198-231 (keep a fixed count)
+// rdmat.h:99-132 (keep a fixed count)
 inline void CarryOverAlphaDet(const std::vector<double>& D, const std::vector<std::vector<size_t>>& adet,
                               size_t kept, std::vector<std::vector<size_t>>& rdet, double& discarded) {
   size_t n = adet.size();

@@ -19,6 +19,11 @@ def test_bounded_wait_gives_up_and_context_survives():
     r0, r1 = (int(x) for x in g["sigma_rows"])
     s = ctx.sigma(C)[r0 * ctx.nb:r1 * ctx.nb]
     assert np.abs(s - g["sigma"]).max() <= 1e-12 * np.abs(g["sigma"]).max()
+    # the tensor-core sigma, whose kernel uses the same wait, also still runs
+    # on this context (its timeout flag starts clear)
+    import sbd_b200
+    stc = ctx.sigma(C, precision=sbd_b200.MIXED_TC)[r0 * ctx.nb:r1 * ctx.nb]
+    assert np.abs(stc - g["sigma"]).max() <= 5e-3 * np.abs(g["sigma"]).max()
 
 
 def test_wait_selftest_rejects_bad_limit():
@@ -26,3 +31,7 @@ def test_wait_selftest_rejects_bad_limit():
     ctx = gpu_ctx(load_golden("g_L8_3e_full"))
     with pytest.raises(sbd_b200.SbdGpuError, match="spin_limit"):
         ctx.wait_selftest(0)
+    # above the kernel's own poll limit (a caller's huge limit would otherwise
+    # make the probe wait for as long as it says)
+    with pytest.raises(sbd_b200.SbdGpuError, match="spin_limit"):
+        ctx.wait_selftest((1 << 26) + 1)

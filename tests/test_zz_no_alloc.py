@@ -9,9 +9,12 @@ done first.
 
 Checked through the C ABI: two calls in a row give the same sigma as the
 regular device-vector entry point (within 1e-12 of max|sigma|, the bar of the
-other sigma tests), a call before the set-up is refused, and a basis above
-the limit is refused before anything runs.  This file is collected last so a
-failure here leaves every other test already run.
+other sigma tests); a call that is the context's very first sigma, right after
+the set-up, leaves the device's free memory unchanged (the array and the
+kernels were loaded when the context was created, not inside the call); a
+call before the set-up is refused, and a basis above the limit is refused
+before anything runs.  This file is collected last so a failure here leaves
+every other test already run.
 """
 import ctypes
 
@@ -32,6 +35,42 @@ def _noalloc(ctx, dC, dS) -> int:
     return lib.sbdgpu_sigma_device_noalloc(ctx._h, ctypes.c_void_p(dC), ctypes.c_void_p(dS))
 
 
+def _unit_vector(n, seed, dev):
+    import torch
+    g = torch.Generator(device=dev).manual_seed(seed)
+    C = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+    return C / torch.linalg.norm(C)
+
+
+def test_noalloc_first_sigma_after_setup_allocates_nothing():
+    import torch
+
+    ints, ne, strs = synth.make_small(10, 3, 100, 21)  # 100 x 100 selected strings
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=0)
+    ctx.tables(0)
+    ctx.hii()
+    dev = torch.device("cuda:0")
+    C = _unit_vector(ctx.n, 5, dev)
+    out = torch.full_like(C, float("nan"))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    assert _noalloc(ctx, C.data_ptr(), out.data_ptr()) == 0  # the context's first sigma
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    # a module load or a scratch allocation inside the call would take at
+    # least one 2 MiB page (the scratch array alone is 12 MiB)
+    assert free0 - free1 < (2 << 20), (free0, free1)
+    ref = torch.empty_like(C)
+    ctx.sigma_device(C.data_ptr(), ref.data_ptr())
+    out2 = torch.full_like(C, float("nan"))
+    assert _noalloc(ctx, C.data_ptr(), out2.data_ptr()) == 0
+    torch.cuda.synchronize()
+    r = ref.cpu().numpy()
+    for o in (out.cpu().numpy(), out2.cpu().numpy()):
+        assert np.all(np.isfinite(o))
+        assert np.abs(o - r).max() <= 1e-12 * np.abs(r).max()
+
+
 def test_noalloc_sigma_matches_regular_entry_point_twice():
     import torch
 
@@ -46,9 +85,7 @@ def test_noalloc_sigma_matches_regular_entry_point_twice():
     ctx.tables(0)
     ctx.hii()
     for seed in (11, 12):
-        g = torch.Generator(device=dev).manual_seed(seed)
-        C = torch.randn(ctx.n, dtype=torch.float64, device=dev, generator=g)
-        C /= torch.linalg.norm(C)
+        C = _unit_vector(ctx.n, seed, dev)
         ref = torch.empty_like(C)
         ctx.sigma_device(C.data_ptr(), ref.data_ptr())
         out = torch.full_like(C, float("nan"))
