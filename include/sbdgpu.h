@@ -105,6 +105,16 @@ int sbdgpu_sigma(sbdgpu_ctx* ctx, const double* C, double* sigma, int precision)
  * after it completes. */
 int sbdgpu_sigma_device(sbdgpu_ctx* ctx, const double* dC, double* dsigma, int precision);
 
+/* Rows [r0, r1) of sigma = H*C, FP64, for the full vector C (device, na*nb
+ * doubles) into sigma_rows (device, (r1-r0)*nb doubles): one rank's share when
+ * W and sigma are split into blocks of alpha rows over several GPUs, the
+ * reference's adet_comm split (chemistry/tpb/helper.h:505-540, ranges from
+ * get_mpi_range, framework/mpi_utility.h:14-36).  The rank gathers C from the
+ * others first (one all-gather per sigma, the counterpart of the reference's
+ * Mpi2dSlide ring, mult.h:440-443, 612-621); every term of its rows is then
+ * summed locally, so no reduction of sigma follows (mult.h:630-631). */
+int sbdgpu_sigma_rows_device(sbdgpu_ctx* ctx, const double* dC, double* dsigma_rows, size_t r0, size_t r1);
+
 /* sigma = H*C with device vectors, for callers that cannot allocate device
  * memory during the call (a pre-reserved memory pool or arena owns the
  * device, or the call sits on a path that must not synchronise the device as

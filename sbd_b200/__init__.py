@@ -27,7 +27,7 @@ EXPORTS = [
     "sbdgpu_sigma", "sbdgpu_sigma_device", "sbdgpu_davidson", "sbdgpu_rdm", "sbdgpu_occupation",
     "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
     "sbdgpu_sigma_device_noalloc", "sbdgpu_store_hamiltonian", "sbdgpu_release_hamiltonian",
-    "sbdgpu_davidson_roots", "sbdgpu_wait_selftest", "sbdgpu_davidson_batch",
+    "sbdgpu_davidson_roots", "sbdgpu_wait_selftest", "sbdgpu_davidson_batch", "sbdgpu_sigma_rows_device",
 ]
 
 
@@ -61,6 +61,7 @@ def lib():
         L.sbdgpu_sigma.argtypes = [_vp, _dp, _dp, ctypes.c_int]
         L.sbdgpu_sigma_device.argtypes = [_vp, _vp, _vp, ctypes.c_int]
         L.sbdgpu_sigma_device_noalloc.argtypes = [_vp, _vp, _vp]
+        L.sbdgpu_sigma_rows_device.argtypes = [_vp, _vp, _vp, ctypes.c_size_t, ctypes.c_size_t]
         L.sbdgpu_davidson.argtypes = [_vp, ctypes.POINTER(Opts), _dp, _dp, _dp, _dp, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_davidson_roots.argtypes = [_vp, ctypes.POINTER(Opts), ctypes.c_int, _dp, _dp, _dp,
@@ -145,6 +146,12 @@ class Context:
 
     def sigma_device(self, dC_ptr: int, dS_ptr: int, precision: int = FP64) -> None:
         self._check(lib().sbdgpu_sigma_device(self._h, _vp(dC_ptr), _vp(dS_ptr), precision))
+
+    def sigma_rows_device(self, dC_ptr: int, dS_ptr: int, r0: int, r1: int) -> None:
+        """FP64 sigma rows [r0, r1) (alpha strings) of the full device vector C
+        into a (r1 - r0) x nb device block: one rank's share of a sigma split
+        into alpha-row blocks."""
+        self._check(lib().sbdgpu_sigma_rows_device(self._h, _vp(dC_ptr), _vp(dS_ptr), int(r0), int(r1)))
 
     def sigma_device_noalloc(self, dC_ptr: int, dS_ptr: int) -> None:
         """FP64 sigma on device vectors that allocates nothing during the call

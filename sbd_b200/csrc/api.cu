@@ -528,6 +528,15 @@ int sbdgpu_sigma_device(sbdgpu_ctx* c, const double* dC, double* dS, int precisi
   });
 }
 
+int sbdgpu_sigma_rows_device(sbdgpu_ctx* c, const double* dC, double* dS, size_t r0, size_t r1) {
+  return guarded(c, [&] {
+    if (!dC || !dS) throw Error{SBDGPU_ERR_ARG, "null vector"};
+    if (r0 > r1 || r1 > c->na) throw Error{SBDGPU_ERR_ARG, "row block outside [0, na]"};
+    if (c->stored) throw Error{SBDGPU_ERR_STATE, "row-block sigma runs on the fly; release the stored Hamiltonian"};
+    sbdgpu::sigma_rows_fp64(c, dC, dS, r0, r1);
+  });
+}
+
 int sbdgpu_last_sigma_ms(sbdgpu_ctx* c, float* ms5) {
   return guarded(c, [&] {
     for (int k = 0; k < 5; k++) ms5[k] = c->last_ms[k];
@@ -703,6 +712,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);
+  cudaFree(c->blk_off); cudaFree(c->blk_idx); cudaFree(c->blk_info);
   cudaFree(c->hii); cudaFree(c->tc_bk_off); cudaFree(c->tc_bk_ent); cudaFree(c->tc_err); cudaFree(c->ct16); cudaFree(c->io32); cudaFree(c->ja32); cudaFree(c->jb32); cudaFree(c->vf32);
   cudaFree(c->io_a); cudaFree(c->io_b); cudaFree(c->ct); cudaFree(c->st); cudaFree(c->red);
   for (int k = 0; k < 8; k++)

@@ -88,6 +88,12 @@ struct sbdgpu_ctx {
   uint32_t* tc_bk_ent = nullptr;
   int* tc_err = nullptr;
   void* ct16 = nullptr;  // BF16 copy of C^T, rows padded to 64 (tensor-core path)
+  // alpha singles restricted to the target rows [blk_r0, blk_r1) (row-block sigma)
+  int64_t* blk_off = nullptr;
+  int32_t* blk_idx = nullptr;
+  uint32_t* blk_info = nullptr;
+  int blk_max = 0;
+  size_t blk_r0 = 0, blk_r1 = 0;
   sbdgpu::SpinTables tab[2];
   // stored Hamiltonian (method 1): off-diagonal elements, CSR by bra determinant
   int64_t* hs_row = nullptr;   // [N+1]
@@ -121,6 +127,7 @@ void free_tables(SpinTables& t);
 void build_j_tables(sbdgpu_ctx* c);
 void compute_hii(sbdgpu_ctx* c);
 void apply_phase(sbdgpu_ctx* c, double* v);
+void apply_phase_rows(sbdgpu_ctx* c, double* v, size_t r0, size_t nrows);  // v: rows r0.. of a vector
 template <typename T>
 void transpose(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s);
 template <typename T>
@@ -167,6 +174,7 @@ void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S);
 void sigma_fp64_prepared(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st);
 void sigma_fp32(sbdgpu_ctx* c, const float* C, float* S);
 void sigma_fp32_tc(sbdgpu_ctx* c, const float* C, float* S);
+void sigma_rows_fp64(sbdgpu_ctx* c, const double* dC, double* S, size_t r0, size_t r1);
 
 // noalloc.cu
 void noalloc_prepare(int device);

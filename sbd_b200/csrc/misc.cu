@@ -456,6 +456,13 @@ void apply_phase(sbdgpu_ctx* c, double* v) {
   SBD_CUDA(cudaGetLastError());
 }
 
+void apply_phase_rows(sbdgpu_ctx* c, double* v, size_t r0, size_t nrows) {
+  if (nrows == 0) return;
+  dim3 g((unsigned)nrows, (unsigned)((c->nb + 255) / 256));
+  phase_kernel<<<g, 256, 0, c->stream>>>(c->astr + r0, c->bstr, c->nb, v);
+  SBD_CUDA(cudaGetLastError());
+}
+
 template <typename T>
 void transpose(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s) {
   dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));

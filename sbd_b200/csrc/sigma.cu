@@ -20,6 +20,7 @@
 // beta singles (sliced ELL, coalesced) once per group, and adds each group's
 // contributions to sigma rows ia with FP64 atomics.
 #include <algorithm>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -32,14 +33,17 @@ constexpr int kRowsCols = 2;  // columns per thread
 
 // sigma_row[ia][cols] (=) diag + sum over the bra's table entries, in the
 // vector type T (double: plain path; float: mixed path, FP32 accumulation).
-// J: [P][ncols] Coulomb coupling to the other spin's occupation.
+// J: [P][jstride] Coulomb coupling to the other spin's occupation.
+// Bra row row0 + blockIdx.x; sigma row blockIdx.x of S (a block of rows when
+// row0 > 0); J rows jstride apart.
 template <typename T, bool kWithDiag>
 __global__ void __launch_bounds__(kRowsThreads) rows_kernel(
     const T* __restrict__ C, T* __restrict__ S, size_t ncols, const double* __restrict__ hii,
     const int64_t* __restrict__ s_off, const int32_t* __restrict__ s_idx, const uint32_t* __restrict__ s_info,
     const double* __restrict__ s_val, const int64_t* __restrict__ d_off, const int32_t* __restrict__ d_idx,
-    const double* __restrict__ d_val, const T* __restrict__ J) {
-  size_t row = blockIdx.x;
+    const double* __restrict__ d_val, const T* __restrict__ J, size_t row0, size_t jstride) {
+  const size_t row = row0 + blockIdx.x;
+  T* Srow = S + (size_t)blockIdx.x * ncols;
   size_t c0 = (size_t)blockIdx.y * (kRowsThreads * kRowsCols) + threadIdx.x;
   T acc[kRowsCols];
   bool ok[kRowsCols];
@@ -55,7 +59,7 @@ __global__ void __launch_bounds__(kRowsThreads) rows_kernel(
     uint32_t info = __ldg(&s_info[k]);
     T v = (T)__ldg(&s_val[k]);
     T sg = (info & 0x80000000u) ? (T)-1 : (T)1;
-    const T* Jr = J + (size_t)((info >> 12) & 0xFFFu) * ncols;
+    const T* Jr = J + (size_t)((info >> 12) & 0xFFFu) * jstride;
     const T* Cr = C + j * ncols;
 #pragma unroll
     for (int u = 0; u < kRowsCols; u++) {
@@ -78,7 +82,7 @@ __global__ void __launch_bounds__(kRowsThreads) rows_kernel(
 #pragma unroll
   for (int u = 0; u < kRowsCols; u++) {
     size_t col = c0 + (size_t)u * kRowsThreads;
-    if (ok[u]) S[row * ncols + col] = acc[u];
+    if (ok[u]) Srow[col] = acc[u];
   }
 }
 
@@ -110,11 +114,11 @@ __global__ void __launch_bounds__(kRowsThreads) rows_vec_kernel(
     const T* __restrict__ C, T* __restrict__ S, size_t ncols, const double* __restrict__ hii,
     const int64_t* __restrict__ s_off, const int32_t* __restrict__ s_idx, const uint32_t* __restrict__ s_info,
     const double* __restrict__ s_val, const int64_t* __restrict__ d_off, const int32_t* __restrict__ d_idx,
-    const double* __restrict__ d_val, const T* __restrict__ J) {
+    const double* __restrict__ d_val, const T* __restrict__ J, size_t row0, size_t jstride) {
   using VT = Vec16<T>;
   using V = typename VT::V;
   constexpr int W = VT::W;
-  const size_t row = blockIdx.x;
+  const size_t row = row0 + blockIdx.x;
   const size_t col = ((size_t)blockIdx.y * kRowsThreads + threadIdx.x) * W;
   if (col >= ncols) return;
   T acc[W];
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(kRowsThreads) rows_vec_kernel(
     const T v = (T)__ldg(&s_val[k]);
     const T sg = (info & 0x80000000u) ? (T)-1 : (T)1;
     T jr[W], cr[W];
-    VT::get(__ldg(reinterpret_cast<const V*>(J + (size_t)((info >> 12) & 0xFFFu) * ncols + col)), jr);
+    VT::get(__ldg(reinterpret_cast<const V*>(J + (size_t)((info >> 12) & 0xFFFu) * jstride + col)), jr);
     VT::get(__ldg(reinterpret_cast<const V*>(C + j * ncols + col)), cr);
 #pragma unroll
     for (int u = 0; u < W; u++) acc[u] += (v + sg * jr[u]) * cr[u];
@@ -150,24 +154,29 @@ __global__ void __launch_bounds__(kRowsThreads) rows_vec_kernel(
 #pragma unroll
     for (int u = 0; u < W; u++) acc[u] += v * cr[u];
   }
-  *reinterpret_cast<V*>(S + row * ncols + col) = VT::make(acc);
+  *reinterpret_cast<V*>(S + (size_t)blockIdx.x * ncols + col) = VT::make(acc);
 }
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 // Same-spin rows: the vector kernel when the rows allow it, else rows_kernel.
+// Bra rows row0 .. row0 + nrows of the table t into the nrows x ncols block S
+// (row0 = 0 and jstride = ncols for a whole vector).
 template <typename T, bool kWithDiag>
 void launch_rows(const T* C, T* S, size_t nrows, size_t ncols, const double* hii, const SpinTables& t, const T* J,
-                 cudaStream_t s) {
+                 cudaStream_t s, size_t row0 = 0, size_t jstride = 0) {
   constexpr int W = Vec16<T>::W;
-  if (ncols % W == 0 && aligned16(C) && aligned16(S) && aligned16(J) && (!kWithDiag || aligned16(hii))) {
+  if (jstride == 0) jstride = ncols;
+  if (nrows == 0) return;
+  if (ncols % W == 0 && jstride % W == 0 && aligned16(C) && aligned16(S) && aligned16(J) &&
+      (!kWithDiag || aligned16(hii))) {
     dim3 g((unsigned)nrows, (unsigned)((ncols / W + kRowsThreads - 1) / kRowsThreads));
     rows_vec_kernel<T, kWithDiag><<<g, kRowsThreads, 0, s>>>(C, S, ncols, hii, t.s_off, t.s_idx, t.s_info, t.s_val,
-                                                             t.d_off, t.d_idx, t.d_val, J);
+                                                             t.d_off, t.d_idx, t.d_val, J, row0, jstride);
   } else {
     dim3 g((unsigned)nrows, (unsigned)((ncols + kRowsThreads * kRowsCols - 1) / (kRowsThreads * kRowsCols)));
     rows_kernel<T, kWithDiag><<<g, kRowsThreads, 0, s>>>(C, S, ncols, hii, t.s_off, t.s_idx, t.s_info, t.s_val,
-                                                         t.d_off, t.d_idx, t.d_val, J);
+                                                         t.d_off, t.d_idx, t.d_val, J, row0, jstride);
   }
   SBD_CUDA(cudaGetLastError());
 }
@@ -212,7 +221,7 @@ __global__ void __launch_bounds__(NT) ab_kernel(
     const T* __restrict__ C, T* __restrict__ S, size_t nb, int P, const T* __restrict__ vf,
     const int64_t* __restrict__ a_off, const int32_t* __restrict__ a_idx, const uint32_t* __restrict__ a_info,
     const int64_t* __restrict__ sell_off, const int32_t* __restrict__ sell_w, const uint32_t* __restrict__ sell,
-    size_t nslice) {
+    size_t nslice, size_t ia0) {
   constexpr int VS = ab_vstride<T, G>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* crow = reinterpret_cast<T*>(smem_raw);  // [nb], padded to 16 bytes
@@ -280,7 +289,7 @@ __global__ void __launch_bounds__(NT) ab_kernel(
     if (ib < nb) {
 #pragma unroll
       for (int g = 0; g < G; g++)
-        if (g < gcount) atomicAdd(&S[(size_t)tgt[g] * nb + ib], sgn[g] * y[g]);
+        if (g < gcount) atomicAdd(&S[((size_t)tgt[g] - ia0) * nb + ib], sgn[g] * y[g]);
     }
   }
 }
@@ -292,22 +301,55 @@ size_t ab_smem(size_t nb, int P) {
 
 // 512 threads while two CTAs fit in shared memory, else 1024 so that one CTA
 // still keeps 32 warps resident per SM.
+// The alpha singles the kernel walks: CSR by source string ja (all targets, or
+// only those of one block of target rows, ia0 .. ia0 + rows).
+struct AlphaSingles {
+  const int64_t* off;
+  const int32_t* idx;
+  const uint32_t* info;
+  int max_s;
+  size_t ia0;
+};
+
 template <typename T, int G>
-void launch_ab(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem) {
-  const SpinTables& ta = c->tab[0];
+void launch_ab(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem, const AlphaSingles& as) {
   const SpinTables& tb = c->tab[1];
-  dim3 grid((unsigned)c->na, (unsigned)((ta.max_s + G - 1) / G));
+  dim3 grid((unsigned)c->na, (unsigned)((as.max_s + G - 1) / G));
   if (grid.y == 0) return;
   if (2 * (smem + 1024) <= 228 * 1024) {
     allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<T, G, 512>), c->device);
-    ab_kernel<T, G, 512><<<grid, 512, smem, c->stream>>>(C, S, c->nb, c->P, vf, ta.s_off, ta.s_idx, ta.s_info,
-                                                         tb.sell_off, tb.sell_w, tb.sell, tb.nslice);
+    ab_kernel<T, G, 512><<<grid, 512, smem, c->stream>>>(C, S, c->nb, c->P, vf, as.off, as.idx, as.info,
+                                                         tb.sell_off, tb.sell_w, tb.sell, tb.nslice, as.ia0);
   } else {
     allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<T, G, 1024>), c->device);
-    ab_kernel<T, G, 1024><<<grid, 1024, smem, c->stream>>>(C, S, c->nb, c->P, vf, ta.s_off, ta.s_idx, ta.s_info,
-                                                           tb.sell_off, tb.sell_w, tb.sell, tb.nslice);
+    ab_kernel<T, G, 1024><<<grid, 1024, smem, c->stream>>>(C, S, c->nb, c->P, vf, as.off, as.idx, as.info,
+                                                           tb.sell_off, tb.sell_w, tb.sell, tb.nslice, as.ia0);
   }
   SBD_CUDA(cudaGetLastError());
+}
+
+// The alpha-beta term: the largest group of alpha singles per CTA whose
+// integral block fits in shared memory next to one row of C.
+template <typename T>
+void alpha_beta(sbdgpu_ctx* c, const T* C, T* S, const T* vf, const AlphaSingles& as) {
+  int dev_smem = 0;
+  SBD_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  size_t budget = (size_t)dev_smem - 1024;
+  if (c->nb > 65536) throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: more than 65536 beta strings"};
+  size_t nb = c->nb;
+  int P = c->P;
+  if (ab_smem<T, 16>(nb, P) <= budget)
+    launch_ab<T, 16>(c, C, S, vf, ab_smem<T, 16>(nb, P), as);
+  else if (ab_smem<T, 8>(nb, P) <= budget)
+    launch_ab<T, 8>(c, C, S, vf, ab_smem<T, 8>(nb, P), as);
+  else if (ab_smem<T, 4>(nb, P) <= budget)
+    launch_ab<T, 4>(c, C, S, vf, ab_smem<T, 4>(nb, P), as);
+  else if (ab_smem<T, 2>(nb, P) <= budget)
+    launch_ab<T, 2>(c, C, S, vf, ab_smem<T, 2>(nb, P), as);
+  else if (ab_smem<T, 1>(nb, P) <= budget)
+    launch_ab<T, 1>(c, C, S, vf, ab_smem<T, 1>(nb, P), as);
+  else
+    throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: one beta row and integral row exceed shared memory"};
 }
 
 // The full kernel sequence of one sigma on given scratch (ct, st: na*nb of T).
@@ -324,24 +366,8 @@ void sigma_launch(sbdgpu_ctx* c, const T* C, T* S, T* ct, T* st, const T* ja, co
   launch_rows<T, false>(ct, st, c->nb, c->na, nullptr, tb, ja, s);
   transpose_add(st, S, c->nb, c->na, s);
   if (events) SBD_CUDA(cudaEventRecord(c->ev[2], s));
-  int dev_smem = 0;
-  SBD_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-  size_t budget = (size_t)dev_smem - 1024;
-  if (c->nb > 65536) throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: more than 65536 beta strings"};
-  size_t nb = c->nb;
-  int P = c->P;
-  if (ab_smem<T, 16>(nb, P) <= budget)
-    launch_ab<T, 16>(c, C, S, vf, ab_smem<T, 16>(nb, P));
-  else if (ab_smem<T, 8>(nb, P) <= budget)
-    launch_ab<T, 8>(c, C, S, vf, ab_smem<T, 8>(nb, P));
-  else if (ab_smem<T, 4>(nb, P) <= budget)
-    launch_ab<T, 4>(c, C, S, vf, ab_smem<T, 4>(nb, P));
-  else if (ab_smem<T, 2>(nb, P) <= budget)
-    launch_ab<T, 2>(c, C, S, vf, ab_smem<T, 2>(nb, P));
-  else if (ab_smem<T, 1>(nb, P) <= budget)
-    launch_ab<T, 1>(c, C, S, vf, ab_smem<T, 1>(nb, P));
-  else
-    throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: one beta row and integral row exceed shared memory"};
+  const SpinTables& tas = c->tab[0];
+  alpha_beta(c, C, S, vf, AlphaSingles{tas.s_off, tas.s_idx, tas.s_info, tas.max_s, 0});
   if (events) SBD_CUDA(cudaEventRecord(c->ev[3], s));
 }
 
@@ -393,6 +419,79 @@ void sigma_fp32(sbdgpu_ctx* c, const float* C, float* S) {
   // the FP64 scratch vectors hold the FP32 transposes (half their size)
   sigma_launch<float>(c, C, S, reinterpret_cast<float*>(c->ct), reinterpret_cast<float*>(c->st), c->ja32, c->jb32,
                       c->vf32, true);
+}
+
+// Alpha singles whose target lies in rows [r0, r1), CSR by source string
+// (kept for the last block asked for).
+void ensure_row_block_singles(sbdgpu_ctx* c, size_t r0, size_t r1) {
+  if (c->blk_off && c->blk_r0 == r0 && c->blk_r1 == r1) return;
+  cudaFree(c->blk_off);
+  cudaFree(c->blk_idx);
+  cudaFree(c->blk_info);
+  c->blk_off = nullptr;
+  c->blk_idx = nullptr;
+  c->blk_info = nullptr;
+  const SpinTables& ta = c->tab[0];
+  std::vector<int32_t> idx(ta.ns);
+  std::vector<uint32_t> info(ta.ns);
+  if (ta.ns) {
+    SBD_CUDA(cudaMemcpy(idx.data(), ta.s_idx, sizeof(int32_t) * ta.ns, cudaMemcpyDeviceToHost));
+    SBD_CUDA(cudaMemcpy(info.data(), ta.s_info, sizeof(uint32_t) * ta.ns, cudaMemcpyDeviceToHost));
+  }
+  std::vector<int64_t> off(c->na + 1, 0);
+  std::vector<int32_t> bidx;
+  std::vector<uint32_t> binfo;
+  int max_s = 0;
+  for (size_t ja = 0; ja < c->na; ja++) {
+    for (int64_t k = ta.h_s_off[ja]; k < ta.h_s_off[ja + 1]; k++)
+      if ((size_t)idx[k] >= r0 && (size_t)idx[k] < r1) {
+        bidx.push_back(idx[k]);
+        binfo.push_back(info[k]);
+      }
+    off[ja + 1] = (int64_t)bidx.size();
+    max_s = std::max(max_s, (int)(off[ja + 1] - off[ja]));
+  }
+  c->blk_off = (int64_t*)dev_alloc(sizeof(int64_t) * off.size());
+  c->blk_idx = (int32_t*)dev_alloc(sizeof(int32_t) * std::max<size_t>(bidx.size(), 1));
+  c->blk_info = (uint32_t*)dev_alloc(sizeof(uint32_t) * std::max<size_t>(binfo.size(), 1));
+  SBD_CUDA(cudaMemcpy(c->blk_off, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice));
+  if (!bidx.empty()) {
+    SBD_CUDA(cudaMemcpy(c->blk_idx, bidx.data(), sizeof(int32_t) * bidx.size(), cudaMemcpyHostToDevice));
+    SBD_CUDA(cudaMemcpy(c->blk_info, binfo.data(), sizeof(uint32_t) * binfo.size(), cudaMemcpyHostToDevice));
+  }
+  c->blk_max = max_s;
+  c->blk_r0 = r0;
+  c->blk_r1 = r1;
+}
+
+// FP64 sigma rows [r0, r1) of H C for the full vector C (device, reference
+// convention) into S_rows ((r1 - r0) x nb, reference convention): the work of
+// one rank when W and sigma are split into blocks of alpha rows (the
+// reference's adet_comm blocks, chemistry/tpb/helper.h:505-540 with
+// get_mpi_range, framework/mpi_utility.h:14-36).  Every term of a target row
+// is summed on this device: alpha rows from C's rows, beta rows from the
+// block's own rows, alpha-beta pairs from the source rows with the singles
+// restricted to the block's targets.
+void sigma_rows_fp64(sbdgpu_ctx* c, const double* dC, double* S, size_t r0, size_t r1) {
+  build_tables(c);
+  compute_hii(c);
+  ensure_scratch(c);
+  ensure_io(c);
+  const size_t nrows = r1 - r0, nb = c->nb;
+  cudaStream_t s = c->stream;
+  const SpinTables& ta = c->tab[0];
+  const SpinTables& tb = c->tab[1];
+  SBD_CUDA(cudaMemcpyAsync(c->io_a, dC, sizeof(double) * c->N, cudaMemcpyDeviceToDevice, s));
+  apply_phase(c, c->io_a);
+  if (nrows == 0) return;
+  launch_rows<double, true>(c->io_a, S, nrows, nb, c->hii, ta, c->jb, s, r0, nb);
+  transpose(c->io_a + r0 * nb, c->ct, nrows, nb, s);
+  launch_rows<double, false>(c->ct, c->st, nb, nrows, nullptr, tb, c->ja + r0, s, 0, c->na);
+  transpose_add(c->st, S, nb, nrows, s);
+  ensure_row_block_singles(c, r0, r1);
+  alpha_beta<double>(c, c->io_a, S, c->vf, AlphaSingles{c->blk_off, c->blk_idx, c->blk_info, c->blk_max, r0});
+  apply_phase_rows(c, S, r0, nrows);
+  SBD_CUDA(cudaStreamSynchronize(s));
 }
 
 // FP32 sigma with the alpha-beta term on the tensor cores (BF16 operands,
