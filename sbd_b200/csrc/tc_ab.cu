@@ -6,23 +6,34 @@
 //
 // For one beta string ib the second line is a dense GEMM: M = folded alpha
 // pair index pq (P = L(L+1)/2 rows, tiles of 128), N = source alpha string ja
-// (tiles of 64), K = the beta singles of ib (chunks of 80).  One CTA owns one
-// ib at a time (persistent over ib), keeps the A operand sb_t (pq|rs_t) for
-// the current K chunk in shared memory, streams B = C[ja, jb_t] tiles from the
-// BF16 transposed vector with cp.async (double buffered), and issues
-// tcgen05.mma from one thread into TMEM (one 128 x 64 FP32 accumulator per M
-// tile).  The epilogue (16 warps, each reading one 32-lane x 16-column block
-// of TMEM with tcgen05.ld) stages one M tile in shared memory and adds the
-// entries that are real alpha singles, prefetched into registers while the
-// MMAs ran, into the CTA's FP32 sigma column with shared-memory atomics; the
-// column is written once per ib into a [nb][na] buffer.
+// (tiles of 64), K = the beta singles of ib (chunks of up to 80).  One
+// persistent CTA per SM takes one ib at a time and runs a warp-specialised
+// pipeline:
+//
+//   warp 0 (one thread)   issues tcgen05.mma into a ring of 8 TMEM
+//                         accumulator stages (one 128 x 64 FP32 tile each)
+//   warps 1-3 (producers) build A = sb_t (pq|rs_t) in BF16 (K-major) once per
+//                         ib and K chunk, and stream B = C[ja, jb_t] tiles
+//                         from the BF16 transposed vector with cp.async into
+//                         two slots (MN-major), completion on mbarriers
+//   warps 4-11 (epilogue) each drain one 32-lane x 32-column block of a stage
+//                         (tcgen05.ld), stage it in a private shared-memory
+//                         tile, release the TMEM stage, and add the entries
+//                         that are real alpha singles into the CTA's FP32
+//                         sigma column with shared-memory atomics; the column
+//                         is written once per ib into a [nb][na] buffer
+//
+// so the MMAs of later tiles overlap the epilogue of earlier ones.  When the A
+// operand of all M tiles does not fit in shared memory (norb 48), the M tiles
+// are taken in groups and the B tiles are streamed once per group.
 //
 // Layouts without swizzle: A is K-major (8-row x 16-byte core matrices,
 // LBO = 128 B between core matrices along K, SBO = 10 x 128 B between 8-row
 // groups); B is MN-major (core matrix = 8 K rows x 8 consecutive ja), so each
 // 16-byte chunk is one cp.async from a row of the transposed vector.  Every
-// wait on the MMA completion barrier is bounded; on timeout the kernel records
-// an error, frees its tensor memory and returns.
+// mbarrier wait is bounded by a poll count and by the global timer; on timeout
+// the kernel records an error, every role stops at its next check, and the CTA
+// frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -34,22 +45,24 @@ namespace sbdgpu {
 
 namespace {
 
-// 16 warps: warp w reads TMEM lane quarter w % 4 and the column group w / 4
-// (kWarpCols columns) of each accumulator in the epilogue
-constexpr int kTcThreads = 512;
+constexpr int kTcThreads = 384;  // warp 0 MMA, warps 1-3 producers, warps 4-11 epilogue
+constexpr int kProdThreads = 96;
+constexpr int kEpiWarps = 8;
+constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kTcN = 64;         // alpha strings (ja) per tile
-constexpr int kTcK = 80;         // beta singles per K chunk (5 MMA steps of 16)
-constexpr int kTcKSteps = kTcK / 16;
+constexpr int kTcK = 80;         // beta singles per K chunk (at most 5 MMA steps of 16)
 constexpr int kTcChunks = kTcK / 8;             // 16-byte core-matrix columns along K
 constexpr uint32_t kLBO = 128;                  // bytes between K-adjacent core matrices
 constexpr uint32_t kSBO = kTcChunks * 128;      // bytes between 8-row groups
-constexpr int kTcMaxMTiles = 8;                 // 8 x 64 = 512 TMEM columns
-constexpr int kWarpCols = kTcN * 4 / (kTcThreads / 32);  // accumulator columns per warp in the epilogue
-static_assert(kWarpCols % 16 == 0 && kWarpCols >= 16, "epilogue reads 16-column groups");
-constexpr int kGStride = kTcN + 4;  // epilogue staging row: 16-byte stores of 8 lanes hit distinct banks
+constexpr int kStages = 8;                      // TMEM accumulator ring: 8 x 64 = 512 columns
+constexpr int kBSlots = 2;                      // B tiles in flight
+constexpr uint32_t kABytesPerMt = 128u * kTcK * 2;   // one M tile of A
+constexpr uint32_t kBBytes = (uint32_t)kTcN * kTcK * 2;  // one B slot
+constexpr int kGS = 36;  // staging row stride (floats): 16-byte stores of 8 lanes hit distinct banks
+constexpr uint32_t kStgBytes = (uint32_t)kEpiWarps * 32 * kGS * 4;
 constexpr long long kSpinLimit = kMaxSpinLimit;
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: an MMA tile completes in microseconds
-constexpr int kEntPerMt = 2;  // bucket entries per thread and M tile prefetched into registers
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: every wait here normally lasts microseconds
+constexpr int kEntPref = 4;  // bucket entries per lane prefetched before a stage's wait
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -127,12 +140,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// One bucket entry: goff | neg<<14 | ia<<15, goff = row * kGStride + column of
-// the staged tile.  sigma[ia] += (-1)^neg G[goff], the sign applied by
-// flipping the float's sign bit.
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(mbar) : "memory");
+}
+
+// arrives on the barrier once every cp.async this thread issued so far has
+// landed (the barrier's expected count includes this arrival)
+__device__ __forceinline__ void cp_async_arrive(uint32_t mbar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void named_sync(int id, int threads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// One bucket entry: goff | neg<<11 | ia<<12, goff = row * kGS + column of the
+// epilogue warp's 32 x 32 staged block.  sigma[ia] += (-1)^neg G[goff], the
+// sign applied by flipping the float's sign bit.
 __device__ __forceinline__ void tc_scatter(const float* G, float* sig, uint32_t en) {
-  const uint32_t g = __float_as_uint(G[en & 0x3FFFu]) ^ ((en << 17) & 0x80000000u);
-  atomicAdd(&sig[en >> 15], __uint_as_float(g));
+  const uint32_t g = __float_as_uint(G[en & 0x7FFu]) ^ ((en << 20) & 0x80000000u);
+  atomicAdd(&sig[en >> 12], __uint_as_float(g));
 }
 
 struct TcArgs {
@@ -142,185 +173,258 @@ struct TcArgs {
   const int64_t* b_off;  // beta singles CSR by bra
   const int32_t* b_idx;
   const uint32_t* b_info;
-  const int64_t* bk_off;   // alpha-pair buckets by (ja tile, M tile)
-  const uint32_t* bk_ent;  // (pq_local * kGStride + ja_local) | neg<<14 | ia<<15
+  const int64_t* bk_off;   // alpha singles bucketed by (ja tile, M tile, epilogue warp)
+  const uint32_t* bk_ent;
   int* err;
-  int na, nb, P, mtiles, na_pad;
+  int na, nb, P, mtiles, na_pad, gsz;  // gsz: M tiles per group (A of a group fits in shared memory)
 };
 
+// The sequence of pipeline stages is the same for every role:
+//   for ib (persistent) / K chunk c / M group g / ja tile / M tile in g.
 __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  constexpr uint32_t kBBytes = (uint32_t)kTcN * kTcK * 2;
-  unsigned char* A = smem_raw;                                      // mtiles x 128 x kTcK bf16, K-major
-  unsigned char* Bb = A + (size_t)a.mtiles * 128 * kTcK * 2;        // 2 x (kTcK x kTcN bf16), MN-major
-  float* G = reinterpret_cast<float*>(Bb + 2 * (size_t)kBBytes);    // 128 x kGStride
-  float* sig = G + 128 * kGStride;                                  // na
+  unsigned char* A = smem_raw;                                           // gsz x 128 x kTcK bf16, K-major
+  unsigned char* Bb = A + (size_t)a.gsz * kABytesPerMt;                  // kBSlots x (kTcK x kTcN bf16)
+  float* stg = reinterpret_cast<float*>(Bb + (size_t)kBSlots * kBBytes); // kEpiWarps x 32 x kGS
+  float* sig = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(stg) + kStgBytes);  // na
   __shared__ int s_jb[kTcK];
   __shared__ int s_rs[kTcK];
   __shared__ float s_sb[kTcK];
-  __shared__ int64_t s_bo[kTcMaxMTiles + 1];
+  __shared__ __align__(8) uint64_t bar_a_full, bar_a_empty, bar_done;
+  __shared__ __align__(8) uint64_t bar_b_full[kBSlots], bar_b_empty[kBSlots];
+  __shared__ __align__(8) uint64_t bar_acc_full[kStages], bar_acc_empty[kStages];
   __shared__ uint32_t s_tmem;
-  __shared__ __align__(8) uint64_t s_mbar;
-  __shared__ int s_fail;
+  __shared__ volatile int s_fail;
+  __shared__ int s_prod_stop, s_epi_stop;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quarter = warp & 3, cgroup = warp >> 2;
-  const uint32_t mbar = smem_addr(&s_mbar);
-  // TMEM columns: a power of two >= 64 per M tile, so small problems leave
-  // room for other CTAs on the SM
-  uint32_t ncols = 32;
-  while (ncols < (uint32_t)(a.mtiles * kTcN)) ncols <<= 1;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
-                 "r"(ncols));
+                 "r"(kStages * kTcN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
+    mbar_init(smem_addr(&bar_a_full), kProdThreads);
+    mbar_init(smem_addr(&bar_a_empty), 1);
+    mbar_init(smem_addr(&bar_done), 1);
+    for (int i = 0; i < kBSlots; i++) {
+      mbar_init(smem_addr(&bar_b_full[i]), kProdThreads);
+      mbar_init(smem_addr(&bar_b_empty[i]), 1);
+    }
+    for (int i = 0; i < kStages; i++) {
+      mbar_init(smem_addr(&bar_acc_full[i]), 1);
+      mbar_init(smem_addr(&bar_acc_empty[i]), kEpiWarps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
+    s_prod_stop = 0;
+    s_epi_stop = 0;
   }
+  for (int i = tid; i < a.na; i += kTcThreads) sig[i] = 0.f;
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
-  uint32_t phase = 0;
   const int ntiles = (a.na + kTcN - 1) / kTcN;
-  const int Mrows = a.mtiles * 128;
-  const uint32_t b_base = smem_addr(Bb);
-
-  // B tile `tile` -> buffer `buf`: 8 chunks of 8 alpha strings per beta single t
-  auto load_b = [&](int tile, int buf) {
-    const int ja0 = tile * kTcN;
-    for (int idx = tid; idx < kTcK * (kTcN / 8); idx += kTcThreads) {
-      int t = idx >> 3, n8 = idx & 7;
-      int jb = s_jb[t];
-      const __nv_bfloat16* src = jb >= 0 ? a.ct16 + (size_t)jb * a.na_pad + ja0 + 8 * n8 : a.ct16;
-      cp_async16(b_base + (uint32_t)buf * kBBytes + mnmajor_chunk_offset(n8, t), src, jb >= 0 ? 16u : 0u);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+  const int ngroups = (a.mtiles + a.gsz - 1) / a.gsz;
+  const uint32_t a_base = smem_addr(A), b_base = smem_addr(Bb);
+  auto fail = [&]() {
+    s_fail = 1;
+    atomicExch(a.err, 1);
   };
 
-  for (int ib = blockIdx.x; ib < a.nb && !s_fail; ib += gridDim.x) {
-    for (int i = tid; i < a.na; i += kTcThreads) sig[i] = 0.f;
-    const int64_t t0 = a.b_off[ib], t1 = a.b_off[ib + 1];
-    for (int64_t kc = t0; kc < t1 && !s_fail; kc += kTcK) {
-      __syncthreads();
-      for (int t = tid; t < kTcK; t += kTcThreads) {
-        int64_t k = kc + t;
-        if (k < t1) {
-          uint32_t info = a.b_info[k];
-          s_jb[t] = a.b_idx[k];
-          s_rs[t] = (info >> 12) & 0xFFFu;
-          s_sb[t] = (info & 0x80000000u) ? -1.f : 1.f;
-        } else {
-          s_jb[t] = -1;
-          s_rs[t] = -1;
-          s_sb[t] = 0.f;
-        }
-      }
-      __syncthreads();
-      load_b(0, 0);
-      // A[m][t] = sb_t (pq_m | rs_t); (pq|rs) is symmetric, so row rs_t of Vf is
-      // read; eight independent loads in flight per thread
-      for (int base = 0; base < Mrows * kTcK; base += 8 * kTcThreads) {
-        float v[8];
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int idx = base + u * kTcThreads + tid;
-          const int t = idx / Mrows, m = idx - t * Mrows;
-          const int rs = idx < Mrows * kTcK ? s_rs[t] : -1;
-          v[u] = (rs >= 0 && m < a.P) ? __ldg(&a.vf[(size_t)rs * a.P + m]) : 0.f;
-        }
-#pragma unroll
-        for (int u = 0; u < 8; u++) {
-          const int idx = base + u * kTcThreads + tid;
-          if (idx < Mrows * kTcK) {
-            const int t = idx / Mrows, m = idx - t * Mrows;
-            *reinterpret_cast<__nv_bfloat16*>(A + kmajor_offset(m, t)) = __float2bfloat16_rn(s_sb[t] * v[u]);
+  if (warp == 0) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      uint32_t stage = 0, tiles_used = 0, a_used = 0;
+      for (int ib = blockIdx.x; ib < a.nb && !s_fail; ib += gridDim.x) {
+        const int64_t nt = a.b_off[ib + 1] - a.b_off[ib];
+        const int nchunk = (int)((nt + kTcK - 1) / kTcK);
+        for (int c = 0; c < nchunk && !s_fail; c++) {
+          const int kt = (int)min((int64_t)kTcK, nt - (int64_t)c * kTcK);
+          const int ksteps = (kt + 15) / 16;
+          for (int g = 0; g < ngroups && !s_fail; g++) {
+            const int mt0 = g * a.gsz, mt1 = min(a.mtiles, mt0 + a.gsz);
+            if (!mbar_wait(smem_addr(&bar_a_full), a_used & 1)) { fail(); break; }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int tile = 0; tile < ntiles && !s_fail; tile++) {
+              const uint32_t slot = tiles_used % kBSlots;
+              if (!mbar_wait(smem_addr(&bar_b_full[slot]), (tiles_used / kBSlots) & 1)) { fail(); break; }
+              asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+              for (int mt = mt0; mt < mt1; mt++) {
+                const uint32_t s = stage % kStages;
+                if (!mbar_wait(smem_addr(&bar_acc_empty[s]), ((stage / kStages) & 1) ^ 1)) { fail(); break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a0 = a_base + (uint32_t)(mt - mt0) * kABytesPerMt;
+                const uint32_t b0 = b_base + slot * kBBytes;
+                for (int ks = 0; ks < ksteps; ks++)
+                  mma_bf16(tmem + s * kTcN, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO),
+                           ks > 0 ? 1u : 0u);
+                mma_commit(smem_addr(&bar_acc_full[s]));
+                stage++;
+              }
+              mma_commit(smem_addr(&bar_b_empty[slot]));
+              tiles_used++;
+            }
+            mma_commit(smem_addr(&bar_a_empty));
+            a_used++;
           }
         }
       }
-      // bucket offsets of the next tile's M tiles, fetched one tile ahead
-      int64_t bo_next = tid <= a.mtiles ? __ldg(&a.bk_off[tid]) : 0;
-      for (int tile = 0; tile < ntiles && !s_fail; tile++) {
-        const int buf = tile & 1;
-        // this tile's bucket offsets (the previous tile's epilogue ended with a
-        // barrier, so nobody still reads the old ones)
-        if (tid <= a.mtiles) s_bo[tid] = bo_next;
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t a0 = smem_addr(A), b0 = b_base + (uint32_t)buf * kBBytes;
-          for (int mt = 0; mt < a.mtiles; mt++)
-#pragma unroll
-            for (int ks = 0; ks < kTcKSteps; ks++)
-              mma_bf16(tmem + (uint32_t)(mt * kTcN), smem_desc(a0 + (uint32_t)mt * 16u * kSBO + ks * 2 * kLBO),
-                       smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
-          mma_commit(mbar);
-        }
-        // the other buffer was read by the previous tile's MMAs, which completed
-        if (tile + 1 < ntiles) load_b(tile + 1, buf ^ 1);
-        if (tile + 1 < ntiles && tid <= a.mtiles) bo_next = __ldg(&a.bk_off[(size_t)(tile + 1) * a.mtiles + tid]);
-        // this tile's bucket entries, loaded while the MMAs run: entry
-        // e = s_bo[mt] + tid + u * kTcThreads of M tile mt in register [mt][u]
-        uint32_t ent[kTcMaxMTiles][kEntPerMt];
-#pragma unroll
-        for (int mt = 0; mt < kTcMaxMTiles; mt++)
-#pragma unroll
-          for (int u = 0; u < kEntPerMt; u++) {
-            const int64_t e = (mt < a.mtiles ? s_bo[mt] : 0) + tid + (int64_t)u * kTcThreads;
-            ent[mt][u] = (mt < a.mtiles && e < s_bo[mt + 1]) ? __ldg(&a.bk_ent[e]) : 0xFFFFFFFFu;
-          }
-        if (!mbar_wait(mbar, phase)) {
-          if (tid == 0) atomicExch(a.err, 1);
-          s_fail = 1;
-        }
-        phase ^= 1u;
-        __syncthreads();
-        if (s_fail) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-        for (int mt = 0; mt < kTcMaxMTiles; mt++) {
-          if (mt >= a.mtiles) break;
-          // TMEM lanes 32q..32q+31 hold rows pq = 128 mt + 32 q + lane; this
-          // warp stages columns [kWarpCols * cgroup, kWarpCols * (cgroup + 1))
-          float v[kWarpCols];
-          const uint32_t trow =
-              tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(mt * kTcN + kWarpCols * cgroup);
-#pragma unroll
-          for (int c16 = 0; c16 < kWarpCols / 16; c16++) tmem_ld16(trow + 16u * c16, v + 16 * c16);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          float4* grow = reinterpret_cast<float4*>(G + (32 * quarter + lane) * kGStride + kWarpCols * cgroup);
-#pragma unroll
-          for (int i = 0; i < kWarpCols / 4; i++) grow[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-          __syncthreads();
-#pragma unroll
-          for (int u = 0; u < kEntPerMt; u++) {
-            const uint32_t en = ent[mt][u];
-            if (en != 0xFFFFFFFFu) tc_scatter(G, sig, en);
-          }
-          // entries beyond the prefetched ones
-          for (int64_t e = s_bo[mt] + tid + (int64_t)kEntPerMt * kTcThreads; e < s_bo[mt + 1]; e += kTcThreads) {
-            tc_scatter(G, sig, __ldg(&a.bk_ent[e]));
-          }
-          __syncthreads();
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      }
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      // every MMA issued has completed before the tensor memory is freed
+      mma_commit(smem_addr(&bar_done));
+      if (!mbar_wait(smem_addr(&bar_done), 0)) fail();
     }
-    __syncthreads();
-    for (int i = tid; i < a.na; i += kTcThreads) a.out[(size_t)ib * a.na + i] = sig[i];
+    __syncwarp();
+  } else if (warp < 4) {
+    // ---------------- producers: A per (ib, chunk, group), B per tile ----------------
+    const int pt = tid - 32;
+    uint32_t tiles_used = 0, a_used = 0;
+    for (int ib = blockIdx.x; ib < a.nb; ib += gridDim.x) {
+      const int64_t t0 = a.b_off[ib], nt = a.b_off[ib + 1] - t0;
+      const int nchunk = (int)((nt + kTcK - 1) / kTcK);
+      for (int c = 0; c < nchunk; c++) {
+        const int kt = (int)min((int64_t)kTcK, nt - (int64_t)c * kTcK);
+        const int krows = (kt + 15) / 16 * 16;
+        named_sync(2, kProdThreads);  // the previous chunk's lists are no longer read
+        for (int t = pt; t < kTcK; t += kProdThreads) {
+          if (t < kt) {
+            const int64_t k = t0 + (int64_t)c * kTcK + t;
+            const uint32_t info = a.b_info[k];
+            s_jb[t] = a.b_idx[k];
+            s_rs[t] = (info >> 12) & 0xFFFu;
+            s_sb[t] = (info & 0x80000000u) ? -1.f : 1.f;
+          } else {
+            s_jb[t] = -1;
+            s_rs[t] = -1;
+            s_sb[t] = 0.f;
+          }
+        }
+        named_sync(2, kProdThreads);
+        for (int g = 0; g < ngroups; g++) {
+          const int mt0 = g * a.gsz, mt1 = min(a.mtiles, mt0 + a.gsz);
+          const int mrows = (mt1 - mt0) * 128;
+          if (!s_fail && !mbar_wait(smem_addr(&bar_a_empty), (a_used & 1) ^ 1)) fail();
+          if (!s_fail) {
+            // A[m][k] = sb_k (pq_m | rs_k): (pq|rs) is symmetric, so row rs_k of
+            // Vf is read, coalesced over m; each task packs 8 consecutive k of
+            // one row m into one 16-byte store
+            const int tasks = mrows * (krows / 8);
+            for (int task = pt; task < tasks; task += kProdThreads) {
+              const int m = task % mrows, k8 = task / mrows;
+              const int pq = mt0 * 128 + m;
+              uint32_t w[4];
+#pragma unroll
+              for (int j = 0; j < 4; j++) {
+                const int k0 = 8 * k8 + 2 * j;
+                const int r0 = s_rs[k0], r1 = s_rs[k0 + 1];
+                const float v0 = (r0 >= 0 && pq < a.P) ? s_sb[k0] * __ldg(&a.vf[(size_t)r0 * a.P + pq]) : 0.f;
+                const float v1 = (r1 >= 0 && pq < a.P) ? s_sb[k0 + 1] * __ldg(&a.vf[(size_t)r1 * a.P + pq]) : 0.f;
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(v0, v1);
+                w[j] = *reinterpret_cast<uint32_t*>(&h2);
+              }
+              *reinterpret_cast<uint4*>(A + kmajor_offset(m, 8 * k8)) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          }
+          mbar_arrive(smem_addr(&bar_a_full));
+          a_used++;
+          for (int tile = 0; tile < ntiles; tile++) {
+            const uint32_t slot = tiles_used % kBSlots;
+            if (!s_fail && !mbar_wait(smem_addr(&bar_b_empty[slot]), ((tiles_used / kBSlots) & 1) ^ 1)) fail();
+            if (!s_fail) {
+              const int ja0 = tile * kTcN;
+              for (int idx = pt; idx < krows * (kTcN / 8); idx += kProdThreads) {
+                const int t = idx >> 3, n8 = idx & 7;
+                const int jb = s_jb[t];
+                const __nv_bfloat16* src = jb >= 0 ? a.ct16 + (size_t)jb * a.na_pad + ja0 + 8 * n8 : a.ct16;
+                cp_async16(b_base + slot * kBBytes + mnmajor_chunk_offset(n8, t), src, jb >= 0 ? 16u : 0u);
+              }
+            }
+            cp_async_arrive(smem_addr(&bar_b_full[slot]));
+            tiles_used++;
+          }
+        }
+      }
+      // a uniform decision among the producers whether to go on
+      named_sync(2, kProdThreads);
+      if (pt == 0) s_prod_stop = s_fail;
+      named_sync(2, kProdThreads);
+      if (s_prod_stop) break;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else {
+    // ---------------- epilogue ----------------
+    const int e = warp - 4, q = e & 3, h = e >> 2;  // TMEM lane quarter = warp % 4
+    float* my = stg + (size_t)e * 32 * kGS;
+    const int et = tid - 128;
+    uint32_t stage = 0;
+    for (int ib = blockIdx.x; ib < a.nb; ib += gridDim.x) {
+      const int64_t nt = a.b_off[ib + 1] - a.b_off[ib];
+      const int nchunk = (int)((nt + kTcK - 1) / kTcK);
+      for (int c = 0; c < nchunk; c++) {
+        for (int g = 0; g < ngroups; g++) {
+          const int mt0 = g * a.gsz, mt1 = min(a.mtiles, mt0 + a.gsz);
+          for (int tile = 0; tile < ntiles; tile++) {
+            for (int mt = mt0; mt < mt1; mt++) {
+              const uint32_t s = stage % kStages;
+              const size_t bk = ((size_t)tile * a.mtiles + mt) * kEpiWarps + e;
+              const int64_t eb = __ldg(&a.bk_off[bk]), ee = __ldg(&a.bk_off[bk + 1]);
+              uint32_t en[kEntPref];
+#pragma unroll
+              for (int j = 0; j < kEntPref; j++) {
+                const int64_t i = eb + lane + 32 * j;
+                en[j] = i < ee ? __ldg(&a.bk_ent[i]) : 0xFFFFFFFFu;
+              }
+              float v[32];
+              bool ok = !s_fail;
+              if (ok && !mbar_wait(smem_addr(&bar_acc_full[s]), (stage / kStages) & 1)) {
+                fail();
+                ok = false;
+              }
+              if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + s * kTcN + 32 * h;
+                tmem_ld16(taddr, v);
+                tmem_ld16(taddr + 16, v + 16);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+              }
+              asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+              __syncwarp();
+              if (lane == 0) mbar_arrive(smem_addr(&bar_acc_empty[s]));  // the stage is free again
+              if (ok) {
+                float4* row = reinterpret_cast<float4*>(my + lane * kGS);
+#pragma unroll
+                for (int i = 0; i < 8; i++) row[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < kEntPref; j++)
+                  if (en[j] != 0xFFFFFFFFu) tc_scatter(my, sig, en[j]);
+                for (int64_t i = eb + lane + 32 * kEntPref; i < ee; i += 32) tc_scatter(my, sig, __ldg(&a.bk_ent[i]));
+                __syncwarp();  // the block is read before the next stage overwrites it
+              }
+              stage++;
+            }
+          }
+        }
+      }
+      // the column of ib is complete: write it out and clear it
+      named_sync(1, kEpiThreads);
+      for (int i = et; i < a.na; i += kEpiThreads) {
+        a.out[(size_t)ib * a.na + i] = sig[i];
+        sig[i] = 0.f;
+      }
+      if (et == 0) s_epi_stop = s_fail;
+      named_sync(1, kEpiThreads);
+      if (s_epi_stop) break;
+    }
   }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kStages * kTcN));
 }
 
 // The bounded mbarrier wait of tc_ab_kernel on its own: one warp waits for
@@ -350,8 +454,22 @@ __global__ void to_bf16_padded_kernel(const float* __restrict__ in, __nv_bfloat1
   }
 }
 
-size_t tc_smem_bytes(int mtiles, size_t na) {
-  return (size_t)mtiles * 128 * kTcK * 2 + 2 * (size_t)kTcN * kTcK * 2 + 128 * kGStride * 4 + na * 4;
+// dynamic shared memory of the kernel with gsz M tiles of A resident
+size_t tc_smem_bytes(int gsz, size_t na) {
+  return (size_t)gsz * kABytesPerMt + (size_t)kBSlots * kBBytes + kStgBytes + ((na * 4 + 15) & ~size_t(15));
+}
+
+// static shared memory of the kernel (lists of one K chunk, barriers, flags)
+constexpr size_t kTcStaticSmem = 3 * kTcK * 4 + (3 + 2 * kBSlots + 2 * kStages) * 8 + 64;
+
+// M tiles per group: as many as fit next to the B slots, the staging blocks
+// and the sigma column (0: not even one fits)
+int tc_group_size(const sbdgpu_ctx* c) {
+  const int mtiles = (c->P + 127) / 128;
+  const size_t budget = 227 * 1024 - kTcStaticSmem - 1024;
+  const size_t fixed = tc_smem_bytes(0, c->na);
+  if (fixed + kABytesPerMt > budget) return 0;
+  return (int)std::min<size_t>((size_t)mtiles, (budget - fixed) / kABytesPerMt);
 }
 
 }  // namespace
@@ -376,42 +494,47 @@ void wait_selftest(sbdgpu_ctx* c, long long limit, int* status) {
 }
 
 bool tc_ab_supported(const sbdgpu_ctx* c) {
-  int mtiles = (c->P + 127) / 128;
-  // na < 2^17: ia takes bits 15..31 of an entry, and an entry of all ones is
-  // the empty-register marker
-  return mtiles <= kTcMaxMTiles && c->na < (1 << 17) - 1 && tc_smem_bytes(mtiles, c->na) <= 225 * 1024;
+  // na < 2^20: ia takes bits 12..31 of a bucket entry (all ones marks an
+  // empty prefetch register); the beta-single pair index has 12 bits
+  return c->na < (1u << 20) - 1 && c->P <= 4096 && tc_group_size(c) >= 1;
 }
 
-// Alpha singles bucketed by (tile of 64 source strings ja, M tile of 128 pq).
+// Alpha singles bucketed by (tile of 64 source strings ja, M tile of 128 pq,
+// epilogue warp: lane quarter q of the M tile and half h of the ja tile).
 void build_tc_buckets(sbdgpu_ctx* c) {
   if (c->tc_bk_ent) return;
   const SpinTables& ta = c->tab[0];
-  int mtiles = (c->P + 127) / 128;
-  size_t na = c->na;
+  const int mtiles = (c->P + 127) / 128;
+  const size_t na = c->na;
   std::vector<int32_t> idx(ta.ns);
   std::vector<uint32_t> info(ta.ns);
   if (ta.ns) {
     SBD_CUDA(cudaMemcpy(idx.data(), ta.s_idx, sizeof(int32_t) * ta.ns, cudaMemcpyDeviceToHost));
     SBD_CUDA(cudaMemcpy(info.data(), ta.s_info, sizeof(uint32_t) * ta.ns, cudaMemcpyDeviceToHost));
   }
-  size_t ntiles = (na + kTcN - 1) / kTcN;
-  std::vector<std::vector<uint32_t>> bucket(ntiles * mtiles);
+  const size_t ntiles = (na + kTcN - 1) / kTcN;
+  const size_t nbk = ntiles * mtiles * kEpiWarps;
+  std::vector<int64_t> off(nbk + 1, 0);
+  auto bucket_of = [&](size_t ja, uint32_t pq) {
+    const uint32_t col = (uint32_t)(ja % kTcN), row = pq % 128u;
+    const uint32_t e = (col / 32u) * 4u + row / 32u;
+    return ((ja / kTcN) * mtiles + pq / 128u) * kEpiWarps + e;
+  };
+  for (size_t ja = 0; ja < na; ja++)
+    for (int64_t k = ta.h_s_off[ja]; k < ta.h_s_off[ja + 1]; k++) off[bucket_of(ja, (info[k] >> 12) & 0xFFFu) + 1]++;
+  for (size_t i = 0; i < nbk; i++) off[i + 1] += off[i];
+  std::vector<uint32_t> ent((size_t)off.back());
+  std::vector<int64_t> pos(off.begin(), off.end() - 1);
   for (size_t ja = 0; ja < na; ja++) {
     for (int64_t k = ta.h_s_off[ja]; k < ta.h_s_off[ja + 1]; k++) {
       // row ja, ket ia: pair index and sign are those of the pair (ia <- ja)
-      uint32_t pq = (info[k] >> 12) & 0xFFFu;
-      uint32_t neg = (info[k] >> 31) & 1u;
-      uint32_t ia = (uint32_t)idx[k];
-      size_t tile = ja / kTcN;
-      uint32_t goff = (pq % 128u) * (uint32_t)kGStride + (uint32_t)(ja % kTcN);  // < 2^14
-      uint32_t e = goff | (neg << 14) | (ia << 15);
-      bucket[tile * mtiles + pq / 128].push_back(e);
+      const uint32_t pq = (info[k] >> 12) & 0xFFFu;
+      const uint32_t neg = (info[k] >> 31) & 1u;
+      const uint32_t ia = (uint32_t)idx[k];
+      const uint32_t goff = (pq % 32u) * (uint32_t)kGS + (uint32_t)(ja % 32u);  // < 2^11
+      ent[(size_t)pos[bucket_of(ja, pq)]++] = goff | (neg << 11) | (ia << 12);
     }
   }
-  std::vector<int64_t> off(bucket.size() + 1, 0);
-  for (size_t i = 0; i < bucket.size(); i++) off[i + 1] = off[i] + (int64_t)bucket[i].size();
-  std::vector<uint32_t> ent((size_t)off.back());
-  for (size_t i = 0; i < bucket.size(); i++) std::copy(bucket[i].begin(), bucket[i].end(), ent.begin() + off[i]);
   c->tc_bk_off = (int64_t*)dev_alloc(sizeof(int64_t) * off.size());
   c->tc_bk_ent = (uint32_t*)dev_alloc(sizeof(uint32_t) * std::max<size_t>(ent.size(), 1));
   SBD_CUDA(cudaMemcpy(c->tc_bk_off, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice));
@@ -446,17 +569,17 @@ void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
   a.nb = (int)c->nb;
   a.P = c->P;
   a.mtiles = (c->P + 127) / 128;
-  size_t smem = tc_smem_bytes(a.mtiles, c->na);
+  a.gsz = tc_group_size(c);
+  if (a.gsz < 1) throw Error{SBDGPU_ERR_LIMIT, "tensor-core alpha-beta kernel: sigma column does not fit"};
+  const size_t smem = tc_smem_bytes(a.gsz, c->na);
   allow_dynamic_smem(reinterpret_cast<const void*>(tc_ab_kernel), c->device);
   int sms = 148;
   SBD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  int grid = (int)std::min<size_t>((size_t)sms, c->nb);
+  const int grid = (int)std::min<size_t>((size_t)sms, c->nb);
   tc_ab_kernel<<<grid, kTcThreads, smem, c->stream>>>(a);
   SBD_CUDA(cudaGetLastError());
 }
 
-// Reads and clears the timeout flag: a timeout is reported once, and the
-// context's later tensor-core sigma builds start clean.
 int tc_error(sbdgpu_ctx* c) {
   if (!c->tc_err) return 0;
   int h = 0;
