@@ -66,7 +66,32 @@ typedef struct sbdgpu_opts {
   int restart_prev; /* mixed precisions only: 1 = also keep the previous step's Ritz
                        vector at a restart (the "+1" of a GD+k restart), with its
                        sigma vector; 0 = not (the reference's behaviour) */
+  int precond;      /* mixed precisions only: SBDGPU_PRECOND_DIAGONAL (the reference's
+                       correction) or SBDGPU_PRECOND_LEARNED */
 } sbdgpu_opts;
+
+/* Davidson correction (sbdgpu_opts.precond). */
+#define SBDGPU_PRECOND_DIAGONAL 0 /* t_i = r_i / (E0 - H_ii), davidson.h:853-862 */
+#define SBDGPU_PRECOND_LEARNED 1  /* t_i = r_i / (E0 - H_ii - s_i), s_i from the context's
+                                     trained network (sbdgpu_precond_train or
+                                     sbdgpu_precond_set); falls back to the diagonal
+                                     correction when the context has no network, or
+                                     for the rest of the run after a restart cycle in
+                                     which the residual norm fell by less than 10 % */
+
+/* Training of the learned preconditioner (no counterpart in the reference). */
+typedef struct sbdgpu_learn_opts {
+  int pairs;      /* (Ritz vector, residual, correction) triples to harvest: one at the
+                     end of each Davidson cycle (FP64, the reference's algorithm) */
+  int cycle;      /* Davidson steps per cycle, 1..32 */
+  int cg_iters;   /* conjugate-gradient steps of each correction solve
+                     (I - uu^T)(H - E0)(I - uu^T) t = -r, t orthogonal to u */
+  int samples;    /* determinants sampled per triple: half with the largest
+                     |t_i|^2 + |r_i|^2, half uniform (weighted), >= 64 */
+  int steps;      /* Adam steps, one whole triple's sample per step */
+  float lr;       /* Adam learning rate */
+  unsigned seed;  /* initial weights and uniform samples */
+} sbdgpu_learn_opts;
 
 /* Create a context on CUDA device `device` for one alpha x beta product basis
  * and Hamiltonian.  Replaces the set-up half of sbd::tpb::diag
@@ -215,6 +240,38 @@ int sbdgpu_last_sigma_ms(sbdgpu_ctx* ctx, float* ms5);
  * stays usable either way.  spin_limit in [1, 2^26] (the kernel's own limit),
  * else SBDGPU_ERR_ARG; each wait also gives up after 2 s of GPU time. */
 int sbdgpu_wait_selftest(sbdgpu_ctx* ctx, long long spin_limit, int* status);
+
+/* Learned preconditioner (no counterpart in the reference; it replaces the
+ * diagonal correction of chemistry/tpb/davidson.h:853-862 when
+ * opts->precond = SBDGPU_PRECOND_LEARNED).  A network of 3 layers (48 features
+ * -> 128 -> 128 -> 1, BF16 weights) maps per-determinant features (H_ii - E0,
+ * |r_i|, holes and particles within 8 orbitals of each spin's Fermi level,
+ * excitation ranks) to a shift s_i of the diagonal denominator.
+ * sbdgpu_precond_train harvests triples on this context's system (on the GPU,
+ * with this library's sigma) and trains the network on them with the
+ * library's own forward and backward kernels.  loss_trace [steps] and
+ * seconds [2] (harvest, training) may be NULL. */
+int sbdgpu_precond_train(sbdgpu_ctx* ctx, const sbdgpu_learn_opts* opts, double* loss_trace, double* seconds);
+
+/* The context's network weights (FP32 master copy): with w == NULL only *n is
+ * set.  A network trained on one system may be loaded into the context of
+ * another with sbdgpu_precond_set (the features do not depend on norb). */
+int sbdgpu_precond_get(sbdgpu_ctx* ctx, float* w, int* n);
+int sbdgpu_precond_set(sbdgpu_ctx* ctx, const float* w, int n);
+
+/* The learned correction of one residual: out_i = R_i / (e0 - H_ii - s_i),
+ * host vectors of na*nb doubles (either sign convention: the network sees
+ * |R_i|).  Runs the tensor-core inference kernel. */
+int sbdgpu_precond_apply(sbdgpu_ctx* ctx, const double* R, double e0, double* out);
+
+/* Loss and gradient of the network's training kernels for master weights w
+ * and B samples with features X [B][48] (FP32), residuals r, denominators
+ * den = E0 - H_ii, Ritz-vector components u, target corrections t and
+ * weights wt, on CUDA device `device` (for checking the kernels' gradients;
+ * S = the shift scale, 0.5 in training). */
+int sbdgpu_mlp_loss_grad(int device, const float* w, int B, const float* X, const double* r, const double* den,
+                         const double* u, const double* t, const double* wt, double S, double eps_reg,
+                         double* loss, float* grad);
 
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);
 void sbdgpu_destroy(sbdgpu_ctx* ctx);

@@ -28,7 +28,12 @@ EXPORTS = [
     "sbdgpu_alpha_weights", "sbdgpu_last_sigma_ms", "sbdgpu_last_error", "sbdgpu_destroy",
     "sbdgpu_sigma_device_noalloc", "sbdgpu_store_hamiltonian", "sbdgpu_release_hamiltonian",
     "sbdgpu_davidson_roots", "sbdgpu_wait_selftest", "sbdgpu_davidson_batch", "sbdgpu_sigma_rows_device",
+    "sbdgpu_precond_train", "sbdgpu_precond_get", "sbdgpu_precond_set", "sbdgpu_precond_apply",
+    "sbdgpu_mlp_loss_grad",
 ]
+
+PRECOND_DIAGONAL = 0
+PRECOND_LEARNED = 1
 
 
 class SbdGpuError(RuntimeError):
@@ -38,7 +43,13 @@ class SbdGpuError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("max_it", ctypes.c_int), ("max_nb", ctypes.c_int), ("eps", ctypes.c_double),
                 ("max_time", ctypes.c_double), ("precision", ctypes.c_int), ("verbose", ctypes.c_int),
-                ("restart_keep", ctypes.c_int), ("restart_prev", ctypes.c_int)]
+                ("restart_keep", ctypes.c_int), ("restart_prev", ctypes.c_int), ("precond", ctypes.c_int)]
+
+
+class LearnOpts(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_int), ("cycle", ctypes.c_int), ("cg_iters", ctypes.c_int),
+                ("samples", ctypes.c_int), ("steps", ctypes.c_int), ("lr", ctypes.c_float),
+                ("seed", ctypes.c_uint)]
 
 
 _lib = None
@@ -70,6 +81,13 @@ def lib():
         L.sbdgpu_davidson_batch.argtypes = [ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(Opts),
                                             ctypes.POINTER(_dp), _dp, ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        _fp = ctypes.POINTER(ctypes.c_float)
+        L.sbdgpu_precond_train.argtypes = [_vp, ctypes.POINTER(LearnOpts), _dp, _dp]
+        L.sbdgpu_precond_get.argtypes = [_vp, _fp, ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_precond_set.argtypes = [_vp, _fp, ctypes.c_int]
+        L.sbdgpu_precond_apply.argtypes = [_vp, _dp, ctypes.c_double, _dp]
+        L.sbdgpu_mlp_loss_grad.argtypes = [ctypes.c_int, _fp, ctypes.c_int, _fp, _dp, _dp, _dp, _dp, _dp,
+                                           ctypes.c_double, ctypes.c_double, _dp, _fp]
         L.sbdgpu_store_hamiltonian.argtypes = [_vp, _u64p]
         L.sbdgpu_release_hamiltonian.argtypes = [_vp]
         L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
@@ -165,7 +183,7 @@ class Context:
         (energies[nroots], W[nroots, n], residual norms, cycles, sigma builds)."""
         W = np.zeros((nroots, self.n)) if W0 is None else np.ascontiguousarray(W0, dtype=np.float64).reshape(
             nroots, self.n).copy()
-        o = Opts(max_it, max_nb, eps, max_time, FP64, verbose, 0, 0)
+        o = Opts(max_it, max_nb, eps, max_time, FP64, verbose, 0, 0, PRECOND_DIAGONAL)
         e = np.zeros(nroots)
         r = np.zeros(nroots)
         it, ns = ctypes.c_int(0), ctypes.c_int(0)
@@ -198,9 +216,9 @@ class Context:
 
     def davidson(self, W0: np.ndarray, max_it: int, max_nb: int, eps: float, max_time: float = 86400.0,
                  precision: int = FP64, verbose: int = 0, max_trace: int = 100000, restart_keep: int = 0,
-                 restart_prev: int = 0):
+                 restart_prev: int = 0, precond: int = PRECOND_DIAGONAL):
         W = np.ascontiguousarray(W0, dtype=np.float64).ravel().copy()
-        o = Opts(max_it, max_nb, eps, max_time, precision, verbose, restart_keep, restart_prev)
+        o = Opts(max_it, max_nb, eps, max_time, precision, verbose, restart_keep, restart_prev, precond)
         e = ctypes.c_double(0.0)
         te = np.zeros(max_trace)
         tt = np.zeros(max_trace)
@@ -209,6 +227,35 @@ class Context:
                                           _p(tt, _dp), max_trace, ctypes.byref(ns)))
         k = min(ns.value, max_trace)
         return e.value, W, te[:k], tt[:k]
+
+    def precond_train(self, pairs: int = 12, cycle: int = 10, cg_iters: int = 40, samples: int = 65536,
+                      steps: int = 600, lr: float = 1e-3, seed: int = 0):
+        """Harvest (Ritz vector, residual, correction) triples on this system
+        and train the learned preconditioner.  Returns (loss per step,
+        [harvest s, training s])."""
+        o = LearnOpts(pairs, cycle, cg_iters, samples, steps, lr, seed)
+        tr = np.zeros(max(steps, 1))
+        sec = np.zeros(2)
+        self._check(lib().sbdgpu_precond_train(self._h, ctypes.byref(o), _p(tr, _dp), _p(sec, _dp)))
+        return tr[:steps], sec
+
+    def precond_get(self) -> np.ndarray:
+        n = ctypes.c_int(0)
+        self._check(lib().sbdgpu_precond_get(self._h, None, ctypes.byref(n)))
+        w = np.zeros(n.value, dtype=np.float32)
+        self._check(lib().sbdgpu_precond_get(self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                             ctypes.byref(n)))
+        return w
+
+    def precond_set(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(lib().sbdgpu_precond_set(self._h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), len(w)))
+
+    def precond_apply(self, R: np.ndarray, e0: float) -> np.ndarray:
+        R = np.ascontiguousarray(R, dtype=np.float64).ravel()
+        out = np.zeros(self.n)
+        self._check(lib().sbdgpu_precond_apply(self._h, _p(R, _dp), float(e0), _p(out, _dp)))
+        return out
 
     def rdm(self, W: np.ndarray):
         W = np.ascontiguousarray(W, dtype=np.float64).ravel()
@@ -239,7 +286,7 @@ def davidson_batch(ctxs, W0s, max_it: int, max_nb: int, eps: float, precision: i
     Ws = [np.ascontiguousarray(w, dtype=np.float64).ravel().copy() for w in W0s]
     hs = (_vp * n)(*[c._h for c in ctxs])
     wp = (_dp * n)(*[_p(w, _dp) for w in Ws])
-    o = Opts(max_it, max_nb, eps, max_time, precision, 0, restart_keep, restart_prev)
+    o = Opts(max_it, max_nb, eps, max_time, precision, 0, restart_keep, restart_prev, PRECOND_DIAGONAL)
     e = np.zeros(n)
     steps = (ctypes.c_int * n)()
     st = (ctypes.c_int * n)()
@@ -251,6 +298,24 @@ def davidson_batch(ctxs, W0s, max_it: int, max_nb: int, eps: float, precision: i
         msg = lib().sbdgpu_last_error(ctxs[bad[0]]._h) if bad else b""
         raise SbdGpuError(f"status {rc} (problems {bad}): {msg.decode() if msg else ''}")
     return e, Ws, [int(x) for x in steps]
+
+
+def mlp_loss_grad(w, X, r, den, u, t, wt, S: float = 0.5, eps_reg: float = 1e-12, device: int = 0):
+    """Loss and gradient of the learned preconditioner's training kernels
+    (sbdgpu_mlp_loss_grad) for master weights w and features X [B, 48]."""
+    fp = ctypes.POINTER(ctypes.c_float)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    vs = [np.ascontiguousarray(v, dtype=np.float64) for v in (r, den, u, t, wt)]
+    B = X.shape[0]
+    loss = ctypes.c_double(0.0)
+    g = np.zeros_like(w)
+    rc = lib().sbdgpu_mlp_loss_grad(int(device), w.ctypes.data_as(fp), B, X.ctypes.data_as(fp),
+                                    *[_p(v, _dp) for v in vs], float(S), float(eps_reg), ctypes.byref(loss),
+                                    g.ctypes.data_as(fp))
+    if rc != 0:
+        raise SbdGpuError(f"sbdgpu_mlp_loss_grad failed with status {rc}")
+    return loss.value, g
 
 
 def context_from_integrals(ints, astr, bstr, device: int = 0) -> Context:

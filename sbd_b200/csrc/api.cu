@@ -251,8 +251,15 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
   // cycles (the projected problem then loses its meaning); a second pass keeps
   // it orthonormal to FP32 rounding.  The collapse restart keeps one pass.
   const int gs_passes = keep > 1 ? 2 : 1;
+  // learned correction while the context has a network and it keeps the
+  // residual falling; the diagonal one otherwise
+  bool use_learned = o->precond == SBDGPU_PRECOND_LEARNED && sbdgpu::learned_ready(c);
+  double tol_learned_cycle = 1e300;
   auto add_correction = [&](int into, double e0) {
-    sbdgpu::precondition(R, c->hii, e0, eps_reg, X, n, st);
+    if (use_learned)
+      sbdgpu::learned_precondition(c, R, e0, eps_reg, X);
+    else
+      sbdgpu::precondition(R, c->hii, e0, eps_reg, X, n, st);
     for (int pass = 0; pass < gs_passes; pass++)
       for (int kb = 0; kb < into; kb++) {
         double olap = sbdgpu::dot_f(c, C[kb], X, C[kb], n);  // <X|C_kb> with X in FP64
@@ -295,6 +302,12 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
       if (tol < o->eps) {
         cont = false;
         break;
+      }
+      if (use_learned && ib == nb - 1) {
+        // fallback: a whole cycle with the learned correction that cut the
+        // residual norm by less than 10 % switches to the diagonal one
+        if (tol > 0.9 * tol_learned_cycle) use_learned = false;
+        tol_learned_cycle = tol;
       }
       if (use_tc) {
         tc_steps++;
@@ -377,8 +390,8 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
       }
     }
   }
-  if (o->precision == SBDGPU_MIXED_TC && sbdgpu::tc_error(c))
-    throw Error{SBDGPU_ERR_CUDA, "tensor-core alpha-beta kernel: completion wait timed out"};
+  if ((o->precision == SBDGPU_MIXED_TC || o->precond == SBDGPU_PRECOND_LEARNED) && sbdgpu::tc_error(c))
+    throw Error{SBDGPU_ERR_CUDA, "tensor-core kernel: completion wait timed out"};
   sbdgpu::sigma_fp64(c, W, R);  // FP64 refinement sigma
   *energy = sbdgpu::dot(c, W, R, n);
   *n_steps = steps;
@@ -548,6 +561,8 @@ int sbdgpu_davidson(sbdgpu_ctx* c, const sbdgpu_opts* o, double* Wh, double* ene
   return guarded(c, [&] {
     if (!o || !Wh) throw Error{SBDGPU_ERR_ARG, "null argument"};
     check_precision(o->precision);
+    if (o->precond != SBDGPU_PRECOND_DIAGONAL && o->precond != SBDGPU_PRECOND_LEARNED)
+      throw Error{SBDGPU_ERR_ARG, "unsupported precond " + std::to_string(o->precond)};
     int nb = o->max_nb;
     if (nb < 1 || nb > 32) throw Error{SBDGPU_ERR_ARG, "max_nb must be in [1, 32]"};
     size_t n = c->N;
@@ -702,6 +717,35 @@ int sbdgpu_alpha_weights(sbdgpu_ctx* c, const double* Wh, double* D) {
   });
 }
 
+int sbdgpu_precond_train(sbdgpu_ctx* c, const sbdgpu_learn_opts* o, double* loss_trace, double* seconds) {
+  return guarded(c, [&] {
+    if (!o) throw Error{SBDGPU_ERR_ARG, "null options"};
+    sbdgpu::train_learned(c, o, loss_trace, seconds);
+  });
+}
+
+int sbdgpu_precond_get(sbdgpu_ctx* c, float* w, int* n) {
+  return guarded(c, [&] { sbdgpu::learned_get(c, w, n); });
+}
+
+int sbdgpu_precond_set(sbdgpu_ctx* c, const float* w, int n) {
+  return guarded(c, [&] { sbdgpu::learned_set(c, w, n); });
+}
+
+int sbdgpu_precond_apply(sbdgpu_ctx* c, const double* Rh, double e0, double* out) {
+  return guarded(c, [&] {
+    if (!Rh || !out) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    sbdgpu::build_tables(c);
+    sbdgpu::compute_hii(c);
+    ensure_io(c);
+    SBD_CUDA(cudaMemcpyAsync(c->io_a, Rh, sizeof(double) * c->N, cudaMemcpyHostToDevice, c->stream));
+    sbdgpu::learned_precondition(c, c->io_a, e0, 1e-12, c->io_b);
+    SBD_CUDA(cudaMemcpyAsync(out, c->io_b, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+    if (sbdgpu::tc_error(c)) throw Error{SBDGPU_ERR_CUDA, "learned preconditioner kernel: wait timed out"};
+  });
+}
+
 const char* sbdgpu_last_error(sbdgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 void sbdgpu_destroy(sbdgpu_ctx* c) {
@@ -709,6 +753,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   sbdgpu::release_hamiltonian(c);
+  sbdgpu::free_learned(c);
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);

@@ -25,6 +25,8 @@
 
 namespace sbdgpu {
 
+struct Learned;  // learned.cu: the preconditioner network of a context
+
 struct Error {
   int code;
   std::string msg;
@@ -88,6 +90,7 @@ struct sbdgpu_ctx {
   uint32_t* tc_bk_ent = nullptr;
   int* tc_err = nullptr;
   void* ct16 = nullptr;  // BF16 copy of C^T, rows padded to 64 (tensor-core path)
+  sbdgpu::Learned* learned = nullptr;  // learned preconditioner, created on first use
   // alpha singles restricted to the target rows [blk_r0, blk_r1) (row-block sigma)
   int64_t* blk_off = nullptr;
   int32_t* blk_idx = nullptr;
@@ -178,6 +181,14 @@ void sigma_rows_fp64(sbdgpu_ctx* c, const double* dC, double* S, size_t r0, size
 
 // noalloc.cu
 void noalloc_prepare(int device);
+
+// learned.cu
+void free_learned(sbdgpu_ctx* c);
+bool learned_ready(const sbdgpu_ctx* c);
+void learned_precondition(sbdgpu_ctx* c, const double* R, double e0, double eps_reg, double* out);
+void train_learned(sbdgpu_ctx* c, const sbdgpu_learn_opts* o, double* loss_trace, double* seconds);
+void learned_get(sbdgpu_ctx* c, float* w, int* n);
+void learned_set(sbdgpu_ctx* c, const float* w, int n);
 
 // api.cu
 void ensure_scratch(sbdgpu_ctx* c);

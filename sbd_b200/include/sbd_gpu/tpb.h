@@ -464,7 +464,8 @@ inline void diag(const MPI_Comm& comm, const SBD& sbd_data, const FCIDump& fcidu
               << ": the GPU path builds H*C on the fly (method 0); results are the same" << std::endl;
   }
   sbdgpu_opts o{sbd_data.max_it,    sbd_data.max_nb, sbd_data.eps,          sbd_data.max_time,
-                sbd_data.precision, 1,               sbd_data.restart_keep, sbd_data.restart_prev};
+                sbd_data.precision, 1,               sbd_data.restart_keep, sbd_data.restart_prev,
+                SBDGPU_PRECOND_DIAGONAL};
   double e = 0.0;
   int steps = 0;
   auto t_dav = std::chrono::high_resolution_clock::now();

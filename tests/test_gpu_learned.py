@@ -1,0 +1,112 @@
+"""Learned Davidson preconditioner on the GPU, against its CPU oracle.
+
+* The training kernels' loss and gradient (forward, loss, backward: every
+  parameter block) equal the float64 restatement in oracle/mlp_oracle.py, on
+  BF16-rounded weights, within FP32 accumulation error.
+* The tensor-core inference kernel gives the oracle's shift s_i on every
+  determinant of a basis (operands rounded to BF16 at the same points).
+* Trained on one system and applied to another of the same shape, the
+  learned correction converges the mixed-precision Davidson to the same
+  energy as the diagonal one; the step counts of both are recorded.  With the
+  diagonal fallback the learned run may not take much longer.
+"""
+import numpy as np
+import pytest
+
+import sbd_b200
+from oracle import mlp_oracle as M
+from sbd_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+S = 0.5
+EPS_REG = 1e-12
+
+
+def _random_batch(B, seed):
+    rng = np.random.default_rng(seed)
+    F = M.feature_width()
+    X = rng.normal(size=(B, F))
+    X[:, 36:] = 0.0
+    r = rng.normal(size=B)
+    den = -rng.uniform(0.05, 3.0, size=B)
+    u = rng.normal(size=B)
+    t = rng.normal(size=B)
+    wt = rng.uniform(0.5, 2.0, size=B)
+    return X.astype(np.float32).astype(np.float64), r, den, u, t, wt
+
+
+def _weights(seed):
+    F = M.feature_width()
+    W1, b1, W2, b2, w3, b3 = M.unpack(M.init_weights(F, seed), F)
+    # an output layer large enough for the shift to matter
+    return M.pack(W1, b1 + 0.05, W2, b2 + 0.05, w3 * 40.0, 0.1).astype(np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("B,seed", [(37, 1), (1000, 2), (4099, 3)])
+def test_training_gradients_match_cpu_oracle(B, seed):
+    F = M.feature_width()
+    w = _weights(seed)
+    X, r, den, u, t, wt = _random_batch(B, seed)
+    loss_ref, g_ref = M.loss_and_grad(w, F, X, r, den, u, t, wt, S, EPS_REG)
+    loss, g = sbd_b200.mlp_loss_grad(w, X, r, den, u, t, wt, S, EPS_REG)
+    assert abs(loss - loss_ref) <= 1e-6 * max(1.0, abs(loss_ref))
+    # every parameter block: W1, b1, W2, b2, w3, b3
+    H = M.HID
+    bounds = [0, H * F, H * F + H, H * F + H + H * H, H * F + 2 * H + H * H, H * F + 3 * H + H * H, len(w)]
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        ref = g_ref[a:b]
+        scale = np.abs(ref).max()
+        assert scale > 0
+        assert np.abs(g[a:b] - ref).max() <= 2e-3 * scale, (a, b)
+
+
+def test_inference_kernel_matches_cpu_oracle():
+    ints, ne, strs = synth.make_small(12, 4, None, 3)  # 495 x 495 = 245,025 determinants
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs)
+    F = M.feature_width()
+    w = _weights(7).astype(np.float32)
+    ctx.precond_set(w)
+    assert np.array_equal(ctx.precond_get(), w)
+    rng = np.random.default_rng(5)
+    R = rng.normal(size=ctx.n)
+    R /= np.linalg.norm(R)
+    hii = ctx.hii()
+    e0 = float(hii.min()) - 0.3
+    out = ctx.precond_apply(R, e0)
+    ia = np.repeat(np.arange(ctx.na), ctx.nb)
+    ib = np.tile(np.arange(ctx.nb), ctx.na)
+    X = M.features(strs, strs, ia, ib, hii, e0, R, ctx.n)
+    z, s_ref, *_ = M.forward(w.astype(np.float64), F, X, S, bf16_acts=True)
+    den = e0 - hii
+    s_gpu = den - R / out
+    err = np.abs(s_gpu - s_ref)
+    assert np.all(np.isfinite(out))
+    assert np.median(err) < 1e-4 and err.max() < 2e-2, (np.median(err), err.max())
+    # odd in R: the network sees |R_i| only
+    np.testing.assert_allclose(ctx.precond_apply(-R, e0), -out, rtol=0, atol=0)
+
+
+def test_trained_network_on_an_unseen_system():
+    """Train on one seeded system, apply to another of the same shape
+    (norb 14, 4 alpha / 4 beta, 600 x 600 selected strings)."""
+    ints_a, ne, strs_a = synth.make_small(14, 4, 600, 21)
+    ctx_a = sbd_b200.context_from_integrals(ints_a, strs_a, strs_a)
+    trace, sec = ctx_a.precond_train(pairs=6, cycle=10, cg_iters=30, samples=16384, steps=240, lr=1e-3, seed=1)
+    assert np.all(np.isfinite(trace))
+    assert trace[-6:].mean() < trace[:6].mean()  # the loss falls over training
+    w = ctx_a.precond_get()
+    ints_b, ne, strs_b = synth.make_small(14, 4, 600, 22)
+    ctx_b = sbd_b200.context_from_integrals(ints_b, strs_b, strs_b)
+    ctx_b.precond_set(w)
+    W0 = np.zeros(ctx_b.n)
+    W0[0] = 1.0
+    e_ref, _, te_ref, _ = ctx_b.davidson(W0, 200, 10, 1e-8)
+    e_d, _, te_d, tt_d = ctx_b.davidson(W0, 200, 10, 1e-4, precision=sbd_b200.MIXED)
+    e_l, _, te_l, tt_l = ctx_b.davidson(W0, 200, 10, 1e-4, precision=sbd_b200.MIXED,
+                                        precond=sbd_b200.PRECOND_LEARNED)
+    print(f"\nunseen system: diagonal {len(te_d)} steps, learned {len(te_l)} steps "
+          f"(FP64 reference {len(te_ref)} steps); harvest {sec[0]:.2f} s, training {sec[1]:.2f} s")
+    assert tt_l[-1] < 1e-4 and tt_d[-1] < 1e-4
+    assert abs(e_l - e_ref) < 1e-6 and abs(e_d - e_ref) < 1e-6
+    assert len(te_l) <= 1.5 * len(te_d) + 10
