@@ -249,7 +249,27 @@ def run_reference(args):
     return 0
 
 
-def time_to_e0(ctx, args):
+def learned_network(args, dev):
+    """The learned preconditioner, trained on the 16M-determinant system
+    (norb 26, 6a/6b, 4,000 strings) on the GPU: triples harvested at the ends
+    of FP64 Davidson cycles, conjugate-gradient correction solves, Adam on the
+    library's own training kernels.  Training time is reported, not counted
+    in the time-to-E0 of the systems it is applied to."""
+    import sbd_b200
+    from sbd_b200 import synth
+    ints, ne, strs = synth.make_workload("c1_L26_6e_4000", seed=0)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    trace, sec = ctx.precond_train(pairs=args.learn_pairs, cycle=10, cg_iters=args.learn_cg, samples=65536,
+                                   steps=args.learn_steps, lr=1e-3, seed=0)
+    w = ctx.precond_get()
+    ctx.close()
+    k = max(1, min(len(trace) // 10, args.learn_pairs))
+    return w, {"trained_on": "c1_L26_6e_4000", "pairs": args.learn_pairs, "cg_iters": args.learn_cg,
+               "steps": args.learn_steps, "harvest_s": float(sec[0]), "train_s": float(sec[1]),
+               "loss_first": float(np.mean(trace[:k])), "loss_last": float(np.mean(trace[-k:]))}
+
+
+def time_to_e0(ctx, args, learned=None):
     """Davidson from the aufbau determinant, plain FP64 against mixed precision.
     The FP64 run goes to a tight residual; its final <W|HW> is the reference
     energy.  Plain time-to-E0 = time of the first step whose Ritz value is
@@ -270,18 +290,31 @@ def time_to_e0(ctx, args):
     k = int(hit[0]) + 1 if len(hit) else len(te)
     t_plain = t_plain_all * k / len(te)
     if not args.time_to_e0:
-        # the default line: the plain run against the fastest mixed mode only
+        # the default line: the plain run against the fastest mixed mode, with
+        # the diagonal and with the learned correction
         t = time.perf_counter()
         e_mp, _, tmp_, ttmp = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED, restart_keep=3,
                                            restart_prev=1)
         t_mp = time.perf_counter() - t
-        return {"method": "mixed FP32 sigma + thick restart (3 Ritz vectors) + previous Ritz vector",
-                "e_fp64": e_ref, "e_mixed": e_mp, "abs_err": abs(e_mp - e_ref), "within_1e-6": abs(e_mp - e_ref) < 1e-6,
-                "plain_steps_total": len(te), "plain_steps_to_1e-6": k, "plain_s_to_1e-6": t_plain,
-                "mixed_steps": len(tmp_), "mixed_s": t_mp, "mixed_final_residual": float(ttmp[-1]),
-                "speedup": t_plain / t_mp, "mixed_tol": args.mixed_tol,
-                "note": "wall-clock seconds (one sigma per step dominates); plain time prorated by steps; "
-                        "--time-to-e0 adds the other mixed modes"}
+        out = {"method": "mixed FP32 sigma + thick restart (3 Ritz vectors) + previous Ritz vector",
+               "e_fp64": e_ref, "e_mixed": e_mp, "abs_err": abs(e_mp - e_ref), "within_1e-6": abs(e_mp - e_ref) < 1e-6,
+               "plain_steps_total": len(te), "plain_steps_to_1e-6": k, "plain_s_to_1e-6": t_plain,
+               "mixed_steps": len(tmp_), "mixed_s": t_mp, "mixed_final_residual": float(ttmp[-1]),
+               "speedup": t_plain / t_mp, "mixed_tol": args.mixed_tol,
+               "note": "wall-clock seconds (one sigma per step dominates); plain time prorated by steps; "
+                       "--time-to-e0 adds the other mixed modes"}
+        if learned is not None:
+            w, info = learned
+            ctx.precond_set(w)
+            t = time.perf_counter()
+            e_l, _, tl, ttl = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED, restart_keep=3,
+                                           restart_prev=1, precond=sbd_b200.PRECOND_LEARNED)
+            t_l = time.perf_counter() - t
+            out["learned"] = {"steps": len(tl), "s": t_l, "e": e_l, "abs_err": abs(e_l - e_ref),
+                              "within_1e-6": abs(e_l - e_ref) < 1e-6, "final_residual": float(ttl[-1]),
+                              "speedup_vs_plain": t_plain / t_l, "speedup_vs_mixed_diagonal": t_mp / t_l,
+                              "network": info}
+        return out
     t = time.perf_counter()
     e_mix, _, tm, ttm = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED)
     t_mixed = time.perf_counter() - t
@@ -352,6 +385,83 @@ def method1_block(args, dev, hbm_peak, peak_kind):
             "note": "12 bytes per stored element (uint32 ket, FP64 value) + row offsets + hii, C, sigma"}
 
 
+def config4_block(args, dev, learned):
+    """The 400M-determinant workload (norb 48, 10a/10b, 20,000 x 20,000
+    selected strings): FP64, FP32 and tensor-core sigma builds per second, and
+    time-to-E0 within 1e-6 Eh for plain FP64, mixed precision with the
+    diagonal correction and with the learned one (the network trained on the
+    16M-determinant system).  FP64 vectors are 3.2 GB each."""
+    import torch
+    import sbd_b200
+    from sbd_b200 import synth
+    ints, ne, strs = synth.make_workload("c4_L48_10e_20000", seed=0)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    n = ctx.n
+    C = torch.randn(n, dtype=torch.float64, device=f"cuda:{dev}",
+                    generator=torch.Generator(device=f"cuda:{dev}").manual_seed(3))
+    C /= torch.linalg.norm(C)
+    S = torch.empty_like(C)
+    out = {"workload": "c4_L48_10e_20000", "determinants": n}
+    for name, prec in (("fp64", sbd_b200.FP64), ("mixed_fp32", sbd_b200.MIXED), ("mixed_tc", sbd_b200.MIXED_TC)):
+        ms = []
+        for i in range(2 + 3):
+            ctx.sigma_device(C.data_ptr(), S.data_ptr(), precision=prec)
+            if i >= 2:
+                ms.append(ctx.last_sigma_ms())
+        out[name] = {"sigma_per_s": 1000.0 * len(ms) / sum(m[3] for m in ms),
+                     "phases_ms": [sum(m[k] for m in ms) / len(ms) for k in range(3)]}
+    del C, S
+    torch.cuda.empty_cache()
+    if args.no_time_to_e0:
+        ctx.close()
+        return out
+    W0 = np.zeros(n)
+    W0[0] = 1.0
+    t = time.perf_counter()
+    e_ref, _, te, tt = ctx.davidson(W0, 100, 10, args.e0_tol, precision=sbd_b200.FP64)
+    t_all = time.perf_counter() - t
+    hit = np.nonzero(te - e_ref < 1e-6)[0]
+    k = int(hit[0]) + 1 if len(hit) else len(te)
+    t_plain = t_all * k / len(te)
+    out["plain"] = {"steps_total": len(te), "steps_to_1e-6": k, "s_to_1e-6": t_plain, "e": e_ref,
+                    "final_residual": float(tt[-1])}
+    t = time.perf_counter()
+    e_m, _, tm, ttm = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED, restart_keep=3,
+                                   restart_prev=1)
+    t_m = time.perf_counter() - t
+    out["mixed"] = {"steps": len(tm), "s": t_m, "abs_err": abs(e_m - e_ref), "within_1e-6": abs(e_m - e_ref) < 1e-6,
+                    "speedup": t_plain / t_m}
+    if learned is not None:
+        ctx.precond_set(learned[0])
+        t = time.perf_counter()
+        e_l, _, tl, ttl = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED, restart_keep=3,
+                                       restart_prev=1, precond=sbd_b200.PRECOND_LEARNED)
+        t_l = time.perf_counter() - t
+        out["learned"] = {"steps": len(tl), "s": t_l, "abs_err": abs(e_l - e_ref),
+                          "within_1e-6": abs(e_l - e_ref) < 1e-6, "speedup": t_plain / t_l,
+                          "speedup_vs_mixed_diagonal": t_m / t_l, "network": learned[1]}
+    ctx.close()
+    return out
+
+
+def rdm_block(args, dev):
+    """1/2-RDMs (sbdgpu_rdm) of a seeded normalised vector on args.rdm_workload,
+    wall-clock including the host copies of the 4 L^4 two-body array."""
+    import sbd_b200
+    from sbd_b200 import synth
+    ints, ne, strs = synth.make_workload(args.rdm_workload, seed=0)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    W = np.random.default_rng(5).normal(size=ctx.n)
+    W /= np.linalg.norm(W)
+    ctx.hii()  # tables and diagonal outside the timing
+    t = time.perf_counter()
+    one, two = ctx.rdm(W)
+    sec = time.perf_counter() - t
+    ctx.close()
+    return {"workload": args.rdm_workload, "determinants": int(len(strs)) ** 2, "seconds": sec,
+            "trace_alpha": float(np.trace(one[:ints.norb ** 2].reshape(ints.norb, ints.norb)))}
+
+
 def roots_block(args, dev):
     """Block Davidson for the lowest args.roots roots (FP64) on the
     16M-determinant system (norb 26, 6a/6b, 4000 x 4000 strings): wall time,
@@ -359,7 +469,7 @@ def roots_block(args, dev):
     FP64 Davidson of the same system."""
     import sbd_b200
     from sbd_b200 import synth
-    ints, ne, strs = synth.make_workload("c1_L26_6e_4000", seed=0)
+    ints, ne, strs = synth.make_workload(args.roots_workload, seed=0)
     ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
     k = args.roots
     nb = min(32, max(2 * k, 3 * k))
@@ -372,7 +482,7 @@ def roots_block(args, dev):
     e1, _, te, _ = ctx.davidson(W0, 200, 10, args.roots_tol)
     t_one = time.perf_counter() - t
     ctx.close()
-    return {"workload": "c1_L26_6e_4000", "roots": k, "max_nb": nb, "eps": args.roots_tol, "seconds": t_block,
+    return {"workload": args.roots_workload, "roots": k, "max_nb": nb, "eps": args.roots_tol, "seconds": t_block,
             "cycles": it, "sigma_builds": ns, "energies": [float(x) for x in E],
             "residuals": [float(x) for x in r], "root0_minus_single_root": float(E[0] - e1),
             "single_root_seconds": t_one, "single_root_steps": len(te)}
@@ -545,12 +655,20 @@ def run_gpu(args):
                      "note": "FP32 vectors; alpha-beta term on tcgen05 tensor cores (BF16 operands, FP32 accumulation)"},
         "clocks": sampler.summary(),
     }
+    learned = None
+    if world == 1 and not args.no_learned and (not args.no_time_to_e0 or args.config4):
+        learned = learned_network(args, dev)
     if world == 1 and not args.no_time_to_e0:
-        line["time_to_e0"] = time_to_e0(ctx, args)
+        line["time_to_e0"] = time_to_e0(ctx, args, learned)
     if not args.no_method1:
         line["method1_stored"] = method1_block(args, dev, hbm_peak, peak_kind)
     if args.roots > 0:
         line["block_roots"] = roots_block(args, dev)
+    if args.rdm:
+        line["rdm"] = rdm_block(args, dev)
+    if args.config4 and world == 1:
+        ctx.close()
+        line["config4"] = config4_block(args, dev, learned)
     if args.batch > 0:
         line["batch"] = batch_block(args, dev)
     if not args.no_cpu_baseline:
@@ -583,7 +701,16 @@ def main():
                     help="time-to-E0 with every mixed mode (by default: plain FP64 against the fastest one)")
     ap.add_argument("--no-time-to-e0", action="store_true", help="skip the time-to-E0 runs")
     ap.add_argument("--no-method1", action="store_true", help="skip the stored-Hamiltonian (method 1) block")
-    ap.add_argument("--roots", type=int, default=0, help="also time block Davidson for this many roots (16M dets)")
+    ap.add_argument("--roots", type=int, default=0, help="also time block Davidson for this many roots")
+    ap.add_argument("--roots-workload", default="c1_L26_6e_4000", help="workload of the block Davidson block")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner run")
+    ap.add_argument("--learn-pairs", type=int, default=12, help="harvested triples for the learned preconditioner")
+    ap.add_argument("--learn-cg", type=int, default=40, help="CG steps per harvested correction")
+    ap.add_argument("--learn-steps", type=int, default=600, help="Adam steps of the learned preconditioner")
+    ap.add_argument("--rdm", action="store_true", help="also time the 1/2-RDMs")
+    ap.add_argument("--rdm-workload", default="c1_L26_6e_4000", help="workload of the RDM block")
+    ap.add_argument("--config4", action="store_true",
+                    help="also run the 400M-determinant workload (norb 48, 10a/10b, 20,000 strings)")
     ap.add_argument("--batch", type=int, default=0, help="also time this many independent small problems at once")
     ap.add_argument("--batch-tol", type=float, default=1e-6, help="residual target of the batched problems")
     ap.add_argument("--roots-tol", type=float, default=1e-5, help="residual target of the block Davidson block")

@@ -366,17 +366,40 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
       for (int c = 0; c < nchunk; c++) {
         for (int g = 0; g < ngroups; g++) {
           const int mt0 = g * a.gsz, mt1 = min(a.mtiles, mt0 + a.gsz);
-          for (int tile = 0; tile < ntiles; tile++) {
-            for (int mt = mt0; mt < mt1; mt++) {
-              const uint32_t s = stage % kStages;
-              const size_t bk = ((size_t)tile * a.mtiles + mt) * kEpiWarps + e;
-              const int64_t eb = __ldg(&a.bk_off[bk]), ee = __ldg(&a.bk_off[bk + 1]);
-              uint32_t en[kEntPref];
+          // stages of this (chunk, group): sidx = tile * gm + (mt - mt0).  The
+          // bucket offsets are loaded two stages ahead and the entries one
+          // stage ahead, so their global-memory latency overlaps the work of
+          // the stages before.
+          const int gm = mt1 - mt0, nst = ntiles * gm;
+          auto bk_of = [&](int sidx) {
+            return ((size_t)(sidx / gm) * a.mtiles + mt0 + sidx % gm) * kEpiWarps + e;
+          };
+          int64_t eb = __ldg(&a.bk_off[bk_of(0)]), ee = __ldg(&a.bk_off[bk_of(0) + 1]);
+          int64_t eb1 = 0, ee1 = 0;
+          if (nst > 1) {
+            eb1 = __ldg(&a.bk_off[bk_of(1)]);
+            ee1 = __ldg(&a.bk_off[bk_of(1) + 1]);
+          }
+          uint32_t en[kEntPref];
+#pragma unroll
+          for (int j = 0; j < kEntPref; j++) {
+            const int64_t i = eb + lane + 32 * j;
+            en[j] = i < ee ? __ldg(&a.bk_ent[i]) : 0xFFFFFFFFu;
+          }
+          for (int sidx = 0; sidx < nst; sidx++) {
+            {
+              uint32_t en_next[kEntPref];
 #pragma unroll
               for (int j = 0; j < kEntPref; j++) {
-                const int64_t i = eb + lane + 32 * j;
-                en[j] = i < ee ? __ldg(&a.bk_ent[i]) : 0xFFFFFFFFu;
+                const int64_t i = eb1 + lane + 32 * j;
+                en_next[j] = (sidx + 1 < nst && i < ee1) ? __ldg(&a.bk_ent[i]) : 0xFFFFFFFFu;
               }
+              int64_t eb2 = 0, ee2 = 0;
+              if (sidx + 2 < nst) {
+                eb2 = __ldg(&a.bk_off[bk_of(sidx + 2)]);
+                ee2 = __ldg(&a.bk_off[bk_of(sidx + 2) + 1]);
+              }
+              const uint32_t s = stage % kStages;
               float v[32];
               bool ok = !s_fail;
               if (ok && !mbar_wait(smem_addr(&bar_acc_full[s]), (stage / kStages) & 1)) {
@@ -405,6 +428,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
                 __syncwarp();  // the block is read before the next stage overwrites it
               }
               stage++;
+              eb = eb1;
+              ee = ee1;
+              eb1 = eb2;
+              ee1 = ee2;
+#pragma unroll
+              for (int j = 0; j < kEntPref; j++) en[j] = en_next[j];
             }
           }
         }
