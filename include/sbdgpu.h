@@ -84,7 +84,7 @@ typedef struct sbdgpu_learn_opts {
   int pairs;      /* (Ritz vector, residual, correction) triples to harvest: one at the
                      end of each Davidson cycle (FP64, the reference's algorithm) */
   int cycle;      /* Davidson steps per cycle, 1..32 */
-  int cg_iters;   /* conjugate-gradient steps of each correction solve
+  int cg_iters;   /* MINRES steps of each correction solve
                      (I - uu^T)(H - E0)(I - uu^T) t = -r, t orthogonal to u */
   int samples;    /* determinants sampled per triple: half with the largest
                      |t_i|^2 + |r_i|^2, half uniform (weighted), >= 64 */

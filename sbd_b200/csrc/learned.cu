@@ -16,8 +16,7 @@
 // Training data are (Ritz vector u, residual r, correction t) triples the
 // method generates itself: at restart points of a Davidson run on the training
 // system, t solves the Jacobi-Davidson correction equation
-// (I - uu^T)(H - E0)(I - uu^T) t = -r by conjugate gradients on this
-// library's own sigma.  (The unprojected (H - E0)^-1 r is u itself, so it
+// (I - uu^T)(H - E0)(I - uu^T) t = -r by MINRES on this library's own sigma.  (The unprojected (H - E0)^-1 r is u itself, so it
 // carries no new direction.)  The loss of one triple is 1 - cos^2(P t_hat, t)
 // over a weighted sample of its determinants, P the projection orthogonal to
 // u.  Training runs on hand-written FP32 kernels (forward, loss, backward,
@@ -761,8 +760,8 @@ void train_learned(sbdgpu_ctx* c, const sbdgpu_learn_opts* o, double* loss_trace
   cudaStream_t st = c->stream;
   const size_t n = c->N;
   auto t_start = std::chrono::steady_clock::now();
-  // working vectors: u, Hu / q, residual (CG), search direction, solution t, r
-  std::vector<double*> vec(6, nullptr);
+  // working vectors: u, Hu / Lanczos, Lanczos (2), solution t, r, two MINRES directions
+  std::vector<double*> vec(8, nullptr);
   struct FreeV {
     std::vector<double*>* v;
     cudaStream_t s;
@@ -818,28 +817,59 @@ void train_learned(sbdgpu_ctx* c, const sbdgpu_learn_opts* o, double* loss_trace
     const double rn = std::sqrt(dot(r, r));
     if (!(rn > 0.0)) throw Error{SBDGPU_ERR_STATE, "harvest: zero residual (converged before the first triple)"};
     scale(r, 1.0 / rn, n, st);
-    // conjugate gradients on (I - uu^T)(H - theta)(I - uu^T) t = -r, t _|_ u
+    // MINRES on (I - uu^T)(H - theta)(I - uu^T) t = -r, t _|_ u: the operator
+    // is symmetric but indefinite while theta is above the lowest eigenvalue,
+    // so conjugate gradients would stop at the first negative curvature.
+    // Lanczos vectors (kept orthogonal to u), the tridiagonal factored by
+    // Givens rotations, t updated along the rotated directions (Paige and
+    // Saunders, SIAM J. Numer. Anal. 12, 1975).  Buffers: vprev, v, p (the
+    // Lanczos recurrence) and w1, w2 (the last two directions); tt holds t.
+    double *vprev = res, *v = p, *pv = q, *w1 = vec[6], *w2 = vec[7];
     SBD_CUDA(cudaMemsetAsync(tt, 0, sizeof(double) * n, st));
-    SBD_CUDA(cudaMemcpyAsync(res, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    scale(res, -1.0, n, st);
-    sub_scaled_kernel<<<592, 256, 0, st>>>(res, u, dot(u, res), n);
-    SBD_CUDA(cudaMemcpyAsync(p, res, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-    double rr = dot(res, res);
-    const double rr0 = rr;
+    SBD_CUDA(cudaMemsetAsync(vprev, 0, sizeof(double) * n, st));
+    SBD_CUDA(cudaMemsetAsync(w1, 0, sizeof(double) * n, st));
+    SBD_CUDA(cudaMemsetAsync(w2, 0, sizeof(double) * n, st));
+    SBD_CUDA(cudaMemcpyAsync(v, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    scale(v, -1.0, n, st);  // b = -r (already orthogonal to u), |b| = 1
+    const double beta1 = std::sqrt(dot(v, v));
+    double beta = beta1, phibar = beta1;
+    double c1 = 1.0, s1 = 0.0, c2 = 1.0, s2 = 0.0;  // rotations k-1 and k-2
+    scale(v, 1.0 / beta1, n, st);
     for (int it = 0; it < o->cg_iters; it++) {
-      sigma_fp64(c, p, q);
-      sub_scaled_kernel<<<592, 256, 0, st>>>(q, p, theta, n);
-      sub_scaled_kernel<<<592, 256, 0, st>>>(q, u, dot(u, q), n);
-      const double pq = dot(p, q);
-      if (!(pq > 0.0)) break;  // (H - theta) not positive on u's complement here
-      const double alpha = rr / pq;
-      axpy(tt, p, alpha, n, st);
-      axpy(res, q, -alpha, n, st);
-      const double rr1 = dot(res, res);
-      if (rr1 < 1e-8 * rr0) break;
-      scale(p, rr1 / rr, n, st);
-      axpy(p, res, 1.0, n, st);
-      rr = rr1;
+      sigma_fp64(c, v, pv);
+      sub_scaled_kernel<<<592, 256, 0, st>>>(pv, v, theta, n);
+      sub_scaled_kernel<<<592, 256, 0, st>>>(pv, u, dot(u, pv), n);
+      if (it > 0) sub_scaled_kernel<<<592, 256, 0, st>>>(pv, vprev, beta, n);
+      const double alpha = dot(v, pv);
+      sub_scaled_kernel<<<592, 256, 0, st>>>(pv, v, alpha, n);
+      const double beta_next = std::sqrt(dot(pv, pv));
+      // column it of the tridiagonal: (beta above, alpha, beta_next below)
+      const double b_above = it > 0 ? beta : 0.0;
+      const double eps_k = s2 * b_above, dbar = c2 * b_above;
+      const double delta = c1 * dbar + s1 * alpha;
+      const double gbar = -s1 * dbar + c1 * alpha;
+      const double gamma = std::sqrt(gbar * gbar + beta_next * beta_next);
+      if (!(gamma > 0.0)) break;
+      const double ck = gbar / gamma, sk = beta_next / gamma;
+      const double tau = ck * phibar;
+      phibar = -sk * phibar;
+      // w_new = (v - delta w1 - eps_k w2) / gamma, built in w2's buffer
+      scale(w2, -eps_k, n, st);
+      axpy(w2, v, 1.0, n, st);
+      axpy(w2, w1, -delta, n, st);
+      scale(w2, 1.0 / gamma, n, st);
+      axpy(tt, w2, tau, n, st);
+      std::swap(w1, w2);
+      c2 = c1;
+      s2 = s1;
+      c1 = ck;
+      s1 = sk;
+      if (std::fabs(phibar) < 1e-4 * beta1 || !(beta_next > 1e-300)) break;
+      // next Lanczos vector
+      scale(pv, 1.0 / beta_next, n, st);
+      std::swap(vprev, v);
+      std::swap(v, pv);
+      beta = beta_next;
     }
     const double tn = std::sqrt(dot(tt, tt));
     if (!(tn > 0.0)) throw Error{SBDGPU_ERR_STATE, "harvest: the correction solve made no progress"};
