@@ -15,13 +15,15 @@
 //   warps 1-3 (producers) build A = sb_t (pq|rs_t) in BF16 (K-major) once per
 //                         ib and K chunk, and stream B = C[ja, jb_t] tiles
 //                         from the BF16 transposed vector with cp.async into
-//                         two slots (MN-major), completion on mbarriers
-//   warps 4-11 (epilogue) each drain one 32-lane x 32-column block of a stage
+//                         four slots (MN-major), completion on mbarriers
+//   warps 4-19 (epilogue) each drain one 32-lane x 16-column block of a stage
 //                         (tcgen05.ld), stage it in a private shared-memory
 //                         tile, release the TMEM stage, and add the entries
-//                         that are real alpha singles into the CTA's FP32
-//                         sigma column with shared-memory atomics; the column
-//                         is written once per ib into a [nb][na] buffer
+//                         that are real alpha singles into the column ib of
+//                         the [nb][na] output with global FP32 reductions
+//                         (native in L2; the CTA's column stays in L2, while
+//                         a float add on shared memory is a compare-and-swap
+//                         loop and measured 1.6x slower for the whole kernel)
 //
 // so the MMAs of later tiles overlap the epilogue of earlier ones.  When the A
 // operand of all M tiles does not fit in shared memory (norb 48), the M tiles
@@ -45,20 +47,21 @@ namespace sbdgpu {
 
 namespace {
 
-constexpr int kTcThreads = 384;  // warp 0 MMA, warps 1-3 producers, warps 4-11 epilogue
+constexpr int kTcThreads = 640;  // warp 0 MMA, warps 1-3 producers, warps 4-19 epilogue
 constexpr int kProdThreads = 96;
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 16;
 constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kTcN = 64;         // alpha strings (ja) per tile
+constexpr int kEpiCols = kTcN * 4 / kEpiWarps;  // accumulator columns per epilogue warp
 constexpr int kTcK = 80;         // beta singles per K chunk (at most 5 MMA steps of 16)
 constexpr int kTcChunks = kTcK / 8;             // 16-byte core-matrix columns along K
 constexpr uint32_t kLBO = 128;                  // bytes between K-adjacent core matrices
 constexpr uint32_t kSBO = kTcChunks * 128;      // bytes between 8-row groups
 constexpr int kStages = 8;                      // TMEM accumulator ring: 8 x 64 = 512 columns
-constexpr int kBSlots = 2;                      // B tiles in flight
+constexpr int kBSlots = 4;                      // B tiles in flight
 constexpr uint32_t kABytesPerMt = 128u * kTcK * 2;   // one M tile of A
 constexpr uint32_t kBBytes = (uint32_t)kTcN * kTcK * 2;  // one B slot
-constexpr int kGS = 36;  // staging row stride (floats): 16-byte stores of 8 lanes hit distinct banks
+constexpr int kGS = kEpiCols;  // staging row stride (floats)
 constexpr uint32_t kStgBytes = (uint32_t)kEpiWarps * 32 * kGS * 4;
 constexpr long long kSpinLimit = kMaxSpinLimit;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: every wait here normally lasts microseconds
@@ -159,16 +162,17 @@ __device__ __forceinline__ void named_sync(int id, int threads) {
 }
 
 // One bucket entry: goff | neg<<11 | ia<<12, goff = row * kGS + column of the
-// epilogue warp's 32 x 32 staged block.  sigma[ia] += (-1)^neg G[goff], the
-// sign applied by flipping the float's sign bit.
-__device__ __forceinline__ void tc_scatter(const float* G, float* sig, uint32_t en) {
+// epilogue warp's 32 x kEpiCols staged block.  col[ia] += (-1)^neg G[goff],
+// the sign applied by flipping the float's sign bit; the add is a global
+// reduction (its result is not read).
+__device__ __forceinline__ void tc_scatter(const float* G, float* col, uint32_t en) {
   const uint32_t g = __float_as_uint(G[en & 0x7FFu]) ^ ((en << 20) & 0x80000000u);
-  atomicAdd(&sig[en >> 12], __uint_as_float(g));
+  atomicAdd(&col[en >> 12], __uint_as_float(g));
 }
 
 struct TcArgs {
   const __nv_bfloat16* ct16;  // C^T in BF16, [nb][na_pad] (zero padded), alpha-string-major convention
-  float* out;            // [nb][na] alpha-beta part of sigma, transposed
+  float* out;            // [nb][na] alpha-beta part of sigma, transposed (zeroed before the launch)
   const float* vf;       // (pq|rs) folded, [P][P]
   const int64_t* b_off;  // beta singles CSR by bra
   const int32_t* b_idx;
@@ -186,7 +190,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
   unsigned char* A = smem_raw;                                           // gsz x 128 x kTcK bf16, K-major
   unsigned char* Bb = A + (size_t)a.gsz * kABytesPerMt;                  // kBSlots x (kTcK x kTcN bf16)
   float* stg = reinterpret_cast<float*>(Bb + (size_t)kBSlots * kBBytes); // kEpiWarps x 32 x kGS
-  float* sig = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(stg) + kStgBytes);  // na
   __shared__ int s_jb[kTcK];
   __shared__ int s_rs[kTcK];
   __shared__ float s_sb[kTcK];
@@ -220,7 +223,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
     s_prod_stop = 0;
     s_epi_stop = 0;
   }
-  for (int i = tid; i < a.na; i += kTcThreads) sig[i] = 0.f;
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -356,13 +358,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else {
     // ---------------- epilogue ----------------
-    const int e = warp - 4, q = e & 3, h = e >> 2;  // TMEM lane quarter = warp % 4
+    const int e = warp - 4, q = e & 3, h = e >> 2;  // TMEM lane quarter = warp % 4, column block h
     float* my = stg + (size_t)e * 32 * kGS;
     const int et = tid - 128;
     uint32_t stage = 0;
     for (int ib = blockIdx.x; ib < a.nb; ib += gridDim.x) {
       const int64_t nt = a.b_off[ib + 1] - a.b_off[ib];
       const int nchunk = (int)((nt + kTcK - 1) / kTcK);
+      float* col = a.out + (size_t)ib * a.na;
       for (int c = 0; c < nchunk; c++) {
         for (int g = 0; g < ngroups; g++) {
           const int mt0 = g * a.gsz, mt1 = min(a.mtiles, mt0 + a.gsz);
@@ -400,7 +403,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
                 ee2 = __ldg(&a.bk_off[bk_of(sidx + 2) + 1]);
               }
               const uint32_t s = stage % kStages;
-              float v[32];
+              float v[kEpiCols];
               bool ok = !s_fail;
               if (ok && !mbar_wait(smem_addr(&bar_acc_full[s]), (stage / kStages) & 1)) {
                 fail();
@@ -408,9 +411,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
               }
               if (ok) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + s * kTcN + 32 * h;
-                tmem_ld16(taddr, v);
-                tmem_ld16(taddr + 16, v + 16);
+                const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + s * kTcN + kEpiCols * h;
+#pragma unroll
+                for (int c16 = 0; c16 < kEpiCols / 16; c16++) tmem_ld16(taddr + 16 * c16, v + 16 * c16);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
               }
               asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -419,12 +422,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
               if (ok) {
                 float4* row = reinterpret_cast<float4*>(my + lane * kGS);
 #pragma unroll
-                for (int i = 0; i < 8; i++) row[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                for (int i = 0; i < kEpiCols / 4; i++) row[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
                 __syncwarp();
 #pragma unroll
                 for (int j = 0; j < kEntPref; j++)
-                  if (en[j] != 0xFFFFFFFFu) tc_scatter(my, sig, en[j]);
-                for (int64_t i = eb + lane + 32 * kEntPref; i < ee; i += 32) tc_scatter(my, sig, __ldg(&a.bk_ent[i]));
+                  if (en[j] != 0xFFFFFFFFu) tc_scatter(my, col, en[j]);
+                for (int64_t i = eb + lane + 32 * kEntPref; i < ee; i += 32) tc_scatter(my, col, __ldg(&a.bk_ent[i]));
                 __syncwarp();  // the block is read before the next stage overwrites it
               }
               stage++;
@@ -438,12 +441,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_ab_kernel(TcArgs a) {
           }
         }
       }
-      // the column of ib is complete: write it out and clear it
+      // a uniform decision among the epilogue warps whether to go on
       named_sync(1, kEpiThreads);
-      for (int i = et; i < a.na; i += kEpiThreads) {
-        a.out[(size_t)ib * a.na + i] = sig[i];
-        sig[i] = 0.f;
-      }
       if (et == 0) s_epi_stop = s_fail;
       named_sync(1, kEpiThreads);
       if (s_epi_stop) break;
@@ -484,19 +483,17 @@ __global__ void to_bf16_padded_kernel(const float* __restrict__ in, __nv_bfloat1
 }
 
 // dynamic shared memory of the kernel with gsz M tiles of A resident
-size_t tc_smem_bytes(int gsz, size_t na) {
-  return (size_t)gsz * kABytesPerMt + (size_t)kBSlots * kBBytes + kStgBytes + ((na * 4 + 15) & ~size_t(15));
-}
+size_t tc_smem_bytes(int gsz) { return (size_t)gsz * kABytesPerMt + (size_t)kBSlots * kBBytes + kStgBytes; }
 
 // static shared memory of the kernel (lists of one K chunk, barriers, flags)
 constexpr size_t kTcStaticSmem = 3 * kTcK * 4 + (3 + 2 * kBSlots + 2 * kStages) * 8 + 64;
 
-// M tiles per group: as many as fit next to the B slots, the staging blocks
-// and the sigma column (0: not even one fits)
+// M tiles per group: as many as fit next to the B slots and the staging
+// blocks (0: not even one fits)
 int tc_group_size(const sbdgpu_ctx* c) {
   const int mtiles = (c->P + 127) / 128;
   const size_t budget = 227 * 1024 - kTcStaticSmem - 1024;
-  const size_t fixed = tc_smem_bytes(0, c->na);
+  const size_t fixed = tc_smem_bytes(0);
   if (fixed + kABytesPerMt > budget) return 0;
   return (int)std::min<size_t>((size_t)mtiles, (budget - fixed) / kABytesPerMt);
 }
@@ -546,7 +543,7 @@ void build_tc_buckets(sbdgpu_ctx* c) {
   std::vector<int64_t> off(nbk + 1, 0);
   auto bucket_of = [&](size_t ja, uint32_t pq) {
     const uint32_t col = (uint32_t)(ja % kTcN), row = pq % 128u;
-    const uint32_t e = (col / 32u) * 4u + row / 32u;
+    const uint32_t e = (col / (uint32_t)kEpiCols) * 4u + row / 32u;
     return ((ja / kTcN) * mtiles + pq / 128u) * kEpiWarps + e;
   };
   for (size_t ja = 0; ja < na; ja++)
@@ -560,7 +557,7 @@ void build_tc_buckets(sbdgpu_ctx* c) {
       const uint32_t pq = (info[k] >> 12) & 0xFFFu;
       const uint32_t neg = (info[k] >> 31) & 1u;
       const uint32_t ia = (uint32_t)idx[k];
-      const uint32_t goff = (pq % 32u) * (uint32_t)kGS + (uint32_t)(ja % 32u);  // < 2^11
+      const uint32_t goff = (pq % 32u) * (uint32_t)kGS + (uint32_t)(ja % kEpiCols);  // < 2^11
       ent[(size_t)pos[bucket_of(ja, pq)]++] = goff | (neg << 11) | (ia << 12);
     }
   }
@@ -583,6 +580,7 @@ void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
   __nv_bfloat16* ct16 = static_cast<__nv_bfloat16*>(c->ct16);
   to_bf16_padded_kernel<<<592, 256, 0, c->stream>>>(ct, ct16, c->nb, c->na, na_pad);
   SBD_CUDA(cudaGetLastError());
+  SBD_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * c->na * c->nb, c->stream));
   TcArgs a;
   a.ct16 = ct16;
   a.na_pad = (int)na_pad;
@@ -599,8 +597,8 @@ void tc_alpha_beta(sbdgpu_ctx* c, const float* ct, float* out) {
   a.P = c->P;
   a.mtiles = (c->P + 127) / 128;
   a.gsz = tc_group_size(c);
-  if (a.gsz < 1) throw Error{SBDGPU_ERR_LIMIT, "tensor-core alpha-beta kernel: sigma column does not fit"};
-  const size_t smem = tc_smem_bytes(a.gsz, c->na);
+  if (a.gsz < 1) throw Error{SBDGPU_ERR_LIMIT, "tensor-core alpha-beta kernel: shared memory too small"};
+  const size_t smem = tc_smem_bytes(a.gsz);
   allow_dynamic_smem(reinterpret_cast<const void*>(tc_ab_kernel), c->device);
   int sms = 148;
   SBD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
