@@ -91,6 +91,12 @@ struct sbdgpu_ctx {
   int* tc_err = nullptr;
   void* ct16 = nullptr;  // BF16 copy of C^T, rows padded to 64 (tensor-core path)
   sbdgpu::Learned* learned = nullptr;  // learned preconditioner, created on first use
+  // dense string-only same-spin operators (FP16 hi/lo, [spin][part]), split
+  // vector scratch and the cuBLAS handle of the mixed-precision sigma
+  void* h0[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  void* c16[2] = {nullptr, nullptr};
+  void* blas = nullptr;
+  bool dense_same_off = false;  // true: same-spin terms from the rows kernels instead
   // alpha singles restricted to the target rows [blk_r0, blk_r1) (row-block sigma)
   int64_t* blk_off = nullptr;
   int32_t* blk_idx = nullptr;
@@ -181,6 +187,12 @@ void sigma_rows_fp64(sbdgpu_ctx* c, const double* dC, double* S, size_t r0, size
 
 // noalloc.cu
 void noalloc_prepare(int device);
+
+// gemm_same.cu
+bool ensure_dense_same(sbdgpu_ctx* c);
+bool use_dense_same(sbdgpu_ctx* c);
+void free_dense_same(sbdgpu_ctx* c);
+void same_spin_dense_fp32(sbdgpu_ctx* c, const float* C, float* S, float* ct, float* st, bool events);
 
 // learned.cu
 void free_learned(sbdgpu_ctx* c);

@@ -417,8 +417,16 @@ void sigma_fp32(sbdgpu_ctx* c, const float* C, float* S) {
   ensure_scratch(c);
   ensure_fp32(c);
   // the FP64 scratch vectors hold the FP32 transposes (half their size)
-  sigma_launch<float>(c, C, S, reinterpret_cast<float*>(c->ct), reinterpret_cast<float*>(c->st), c->ja32, c->jb32,
-                      c->vf32, true);
+  float* ct = reinterpret_cast<float*>(c->ct);
+  float* st = reinterpret_cast<float*>(c->st);
+  if (use_dense_same(c)) {
+    same_spin_dense_fp32(c, C, S, ct, st, true);
+    const SpinTables& ta = c->tab[0];
+    alpha_beta<float>(c, C, S, c->vf32, AlphaSingles{ta.s_off, ta.s_idx, ta.s_info, ta.max_s, 0});
+    SBD_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    return;
+  }
+  sigma_launch<float>(c, C, S, ct, st, c->ja32, c->jb32, c->vf32, true);
 }
 
 // Alpha singles whose target lies in rows [r0, r1), CSR by source string
@@ -508,13 +516,17 @@ void sigma_fp32_tc(sbdgpu_ctx* c, const float* C, float* S) {
   cudaStream_t s = c->stream;
   float* ct = reinterpret_cast<float*>(c->ct);
   float* st = reinterpret_cast<float*>(c->st);
-  SBD_CUDA(cudaEventRecord(c->ev[0], s));
-  launch_rows<float, true>(C, S, c->na, c->nb, c->hii, ta, c->jb32, s);
-  SBD_CUDA(cudaEventRecord(c->ev[1], s));
-  transpose(C, ct, c->na, c->nb, s);
-  launch_rows<float, false>(ct, st, c->nb, c->na, nullptr, tb, c->ja32, s);
-  transpose_add(st, S, c->nb, c->na, s);
-  SBD_CUDA(cudaEventRecord(c->ev[2], s));
+  if (use_dense_same(c)) {
+    same_spin_dense_fp32(c, C, S, ct, st, true);  // leaves C^T in ct
+  } else {
+    SBD_CUDA(cudaEventRecord(c->ev[0], s));
+    launch_rows<float, true>(C, S, c->na, c->nb, c->hii, ta, c->jb32, s);
+    SBD_CUDA(cudaEventRecord(c->ev[1], s));
+    transpose(C, ct, c->na, c->nb, s);
+    launch_rows<float, false>(ct, st, c->nb, c->na, nullptr, tb, c->ja32, s);
+    transpose_add(st, S, c->nb, c->na, s);
+    SBD_CUDA(cudaEventRecord(c->ev[2], s));
+  }
   tc_alpha_beta(c, ct, st);
   transpose_add(st, S, c->nb, c->na, s);
   SBD_CUDA(cudaEventRecord(c->ev[3], s));

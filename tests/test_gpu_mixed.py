@@ -54,3 +54,29 @@ def test_mixed_thick_restart(golden):
     # the previous vector alone with the collapse restart
     e5, _, t5, tt5 = ctx.davidson(W0, 1000, 10, 1e-5, precision=sbd_b200.MIXED, restart_prev=1)
     assert abs(e5 - float(golden["energy"])) < 1e-6 and tt5[-1] < 1e-5
+
+
+@pytest.mark.parametrize("norb,ne,count,seed", [(16, 5, 1100, 31), (18, 4, 1500, 32)])
+def test_mixed_sigma_dense_same_spin(norb, ne, count, seed):
+    """From 1,024 strings per spin the FP32 sigma takes its same-spin terms from
+    dense split-FP16 tensor-core products (the string-only operator) plus the
+    singles' Coulomb part and the diagonal from a rows kernel: FP32-class
+    against the FP64 sigma, and its Davidson lands on the FP64 energy."""
+    import sbd_b200
+    from sbd_b200 import synth
+    from conftest import seeded_vector
+    ints, ne, strs = synth.make_small(norb, ne, count, seed)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs)
+    C = seeded_vector(ctx.n, seed)
+    s64 = ctx.sigma(C)
+    s32 = ctx.sigma(C, precision=sbd_b200.MIXED)
+    assert np.abs(s32 - s64).max() <= 2e-5 * np.abs(s64).max()
+    # an unnormalised vector (the FP16 split rescales by a power of two)
+    s32b = ctx.sigma(1e3 * C, precision=sbd_b200.MIXED)
+    assert np.abs(s32b - 1e3 * s64).max() <= 2e-5 * 1e3 * np.abs(s64).max()
+    W0 = np.random.default_rng(seed).normal(size=ctx.n)
+    W0 *= 0.01 / np.linalg.norm(W0)
+    W0[0] += 1.0
+    e64, _, _, _ = ctx.davidson(W0, 200, 10, 1e-7)
+    e32, _, _, tt = ctx.davidson(W0, 200, 10, 1e-4, precision=sbd_b200.MIXED, restart_keep=3, restart_prev=1)
+    assert tt[-1] < 1e-4 and abs(e32 - e64) < 1e-6
