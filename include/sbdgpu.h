@@ -276,6 +276,69 @@ int sbdgpu_mlp_loss_grad(int device, const float* w, int B, const float* X, cons
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);
 void sbdgpu_destroy(sbdgpu_ctx* ctx);
 
+/* ---- The generic path: a second-quantised operator on a basis of bit strings
+ * (basic/generalop.h GeneralOp, basic/basis.h Basis,
+ * basic/out_of_place_func/mult.h, lanczos.h, davidson.h). ---- */
+
+typedef struct sbdgpu_genop sbdgpu_genop;
+
+/* Maximum field operators in one term, and words (64 sites each) per state. */
+#define SBDGPU_GENOP_MAX_OPS 16
+#define SBDGPU_GENOP_MAX_WORDS 4
+
+/* A basis of nstates bit strings on CUDA device `device`: state i is
+ * states[i*nwords .. i*nwords+nwords), site q at bit q%64 of word q/64
+ * (1 <= nwords <= 4).  Any order; vectors follow it.  A repeated state is
+ * refused (SBDGPU_ERR_ARG).  sign = 1: fermionic signs (each operator counts
+ * the occupied sites below its own, basic/out_of_place_func/mult.h:213-240 with
+ * framework/bit_manipulation.h:943-962); 0: none.  Replaces Basis::Init
+ * (basis.h:208-256) at one rank.  Copies all inputs. */
+int sbdgpu_genop_create(sbdgpu_genop** out, int device, int nwords, size_t nstates, const uint64_t* states,
+                        int sign);
+
+/* The operator, as GeneralOp keeps it (generalop.h:17-826): n_diag terms of
+ * the diagonal list (d_, e_) and n_off of the off-diagonal list (o_, c_).
+ * Term k of a list has the field operators ops[off[k] .. off[k+1]) in the
+ * order written, each site | dag << 16, n_dag[k] of them creation operators
+ * (ProductOp::n_dag), coefficient coef[k].  As in mult.h:118-144 a diagonal
+ * term adds coef * C_i where the sites of its first n_dag operators are all
+ * occupied; as in mult.h:207-256 an off-diagonal term annihilates the sites of
+ * its first n_dag operators from the bra state in turn and creates those of
+ * the rest, and adds coef * sign * C_j when the result is basis state j.
+ * Replaces any earlier operator.  At most SBDGPU_GENOP_MAX_OPS operators per
+ * term, sites below 64 * nwords. */
+int sbdgpu_genop_set_terms(sbdgpu_genop* g, size_t n_diag, const int64_t* diag_off, const int32_t* diag_ops,
+                           const int32_t* diag_ndag, const double* diag_coef, size_t n_off, const int64_t* off_off,
+                           const int32_t* off_ops, const int32_t* off_ndag, const double* off_coef);
+
+/* W += H C (mult.h:268-291 at one rank: the diagonal list, then the
+ * off-diagonal one).  Host vectors of nstates doubles; the _device form takes
+ * device pointers and runs on the object's stream. */
+int sbdgpu_genop_mult(sbdgpu_genop* g, const double* C, double* W);
+int sbdgpu_genop_mult_device(sbdgpu_genop* g, const double* dC, double* dW);
+
+/* <i|H|i> for every basis state (the diagonal terms plus the off-diagonal ones
+ * that map a state onto itself). */
+int sbdgpu_genop_diagonal(sbdgpu_genop* g, double* hii);
+
+/* Lanczos for the lowest eigenvalue (lanczos.h:176-310): W (normalised) is the
+ * start vector and receives the Ritz vector, rebuilt by a second pass of the
+ * recurrence; stops when the lowest Ritz value moves by less than eps, when a
+ * new Lanczos coefficient is below eps, or after max_it steps.  *energy = the
+ * lowest Ritz value; *n_iter = Lanczos steps taken.  No reorthogonalisation,
+ * as in the reference. */
+int sbdgpu_genop_lanczos(sbdgpu_genop* g, double* W, int max_it, double eps, double* energy, int* n_iter);
+
+/* Davidson for the lowest eigenvalue with on-the-fly sigma (the algorithm of
+ * basic/out_of_place_func/davidson.h:19-196 and chemistry/tpb/davidson.h:
+ * collapse restart, diagonal correction r_i / (E0 - H_ii)); opts->max_it,
+ * max_nb, eps, verbose are used.  Traces as sbdgpu_davidson. */
+int sbdgpu_genop_davidson(sbdgpu_genop* g, const sbdgpu_opts* opts, double* W, double* energy, double* trace_e,
+                          double* trace_tol, int max_trace, int* n_steps);
+
+const char* sbdgpu_genop_last_error(sbdgpu_genop* g);
+void sbdgpu_genop_destroy(sbdgpu_genop* g);
+
 #ifdef __cplusplus
 }
 #endif

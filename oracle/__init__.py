@@ -28,7 +28,9 @@ _dp = ctypes.POINTER(ctypes.c_double)
 def build() -> None:
     """Compile the checkers (make in oracle/; the reference part only where the
     reference checkout exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    ref = "/root/reference"  # the reference checkout, where this machine has one
+    args = ["make", "-s", "-C", HERE] + ([f"REF={ref}"] if os.path.exists(os.path.join(ref, "include")) else [])
+    subprocess.run(args, check=True)
 
 
 def _ptr(a, t):
@@ -293,3 +295,79 @@ def phase(astr: np.ndarray, bstr: np.ndarray) -> np.ndarray:
         bc = np.array([bin(int(x) & int(mask)).count("1") for x in (b & mask)], dtype=np.int64)
         cnt += ap[:, None] * bc[None, :]
     return np.where(cnt % 2 == 1, -1.0, 1.0)
+
+
+REF_GENERIC_SO = os.path.join(HERE, "_ref", "libsbdref_generic.so")
+
+
+class RefGeneric:
+    """The reference's own generic operator algebra (basic/): GeneralOp built
+    with its operators, NormalOrdering, Simplify and GeneralOp_From_FCIDump,
+    exported as (diagonal, off-diagonal) lists of (coef, [(dag, site), ...])."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = ctypes.CDLL(REF_GENERIC_SO)
+            vp = ctypes.c_void_p
+            ip = ctypes.POINTER(ctypes.c_int)
+            lib.sbdrefg_new.restype = vp
+            lib.sbdrefg_free.argtypes = [vp]
+            lib.sbdrefg_add_product.argtypes = [vp, ctypes.c_double, ctypes.c_int, ip]
+            lib.sbdrefg_normal_order.argtypes = [vp, ctypes.c_int]
+            lib.sbdrefg_simplify.argtypes = [vp]
+            lib.sbdrefg_from_fcidump.restype = vp
+            lib.sbdrefg_from_fcidump.argtypes = [ctypes.c_char_p, ip, ip]
+            lib.sbdrefg_count.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
+                                          ctypes.POINTER(ctypes.c_size_t)]
+            lib.sbdrefg_export.argtypes = [vp, ctypes.c_int, _dp, ip, ctypes.POINTER(ctypes.c_int64), ip]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, handle=None):
+        self.h = handle if handle is not None else self.lib().sbdrefg_new()
+
+    @classmethod
+    def from_fcidump(cls, path: str):
+        L, N = ctypes.c_int(0), ctypes.c_int(0)
+        h = cls.lib().sbdrefg_from_fcidump(path.encode(), ctypes.byref(L), ctypes.byref(N))
+        return cls(h), L.value, N.value
+
+    def close(self):
+        if self.h:
+            self.lib().sbdrefg_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, coef: float, ops):
+        arr = np.asarray([int(q) | (0x10000 if d else 0) for d, q in ops] or [0], dtype=np.int32)
+        self.lib().sbdrefg_add_product(self.h, float(coef), len(ops), arr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+
+    def normal_order(self, sign: bool = True):
+        self.lib().sbdrefg_normal_order(self.h, 1 if sign else 0)
+
+    def simplify(self):
+        self.lib().sbdrefg_simplify(self.h)
+
+    def terms(self):
+        out = []
+        for lst in (0, 1):
+            nt, no = ctypes.c_size_t(0), ctypes.c_size_t(0)
+            self.lib().sbdrefg_count(self.h, lst, ctypes.byref(nt), ctypes.byref(no))
+            coef = np.zeros(max(nt.value, 1))
+            ndag = np.zeros(max(nt.value, 1), dtype=np.int32)
+            off = np.zeros(nt.value + 1, dtype=np.int64)
+            ops = np.zeros(max(no.value, 1), dtype=np.int32)
+            ip = ctypes.POINTER(ctypes.c_int)
+            self.lib().sbdrefg_export(self.h, lst, coef.ctypes.data_as(_dp), ndag.ctypes.data_as(ip),
+                                      off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ops.ctypes.data_as(ip))
+            out.append([(float(coef[m]), [(bool(x >> 16 & 1), int(x & 0xFFFF)) for x in ops[off[m]:off[m + 1]]])
+                        for m in range(nt.value)])
+        return out[0], out[1]

@@ -29,7 +29,9 @@ EXPORTS = [
     "sbdgpu_sigma_device_noalloc", "sbdgpu_store_hamiltonian", "sbdgpu_release_hamiltonian",
     "sbdgpu_davidson_roots", "sbdgpu_wait_selftest", "sbdgpu_davidson_batch", "sbdgpu_sigma_rows_device",
     "sbdgpu_precond_train", "sbdgpu_precond_get", "sbdgpu_precond_set", "sbdgpu_precond_apply",
-    "sbdgpu_mlp_loss_grad",
+    "sbdgpu_mlp_loss_grad", "sbdgpu_genop_create", "sbdgpu_genop_set_terms", "sbdgpu_genop_mult",
+    "sbdgpu_genop_mult_device", "sbdgpu_genop_diagonal", "sbdgpu_genop_lanczos", "sbdgpu_genop_davidson",
+    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy",
 ]
 
 PRECOND_DIAGONAL = 0
@@ -97,6 +99,21 @@ def lib():
         L.sbdgpu_last_error.restype = ctypes.c_char_p
         L.sbdgpu_last_error.argtypes = [_vp]
         L.sbdgpu_destroy.argtypes = [_vp]
+        _i64p, _i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+        L.sbdgpu_genop_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_size_t, _u64p,
+                                          ctypes.c_int]
+        L.sbdgpu_genop_set_terms.argtypes = [_vp, ctypes.c_size_t, _i64p, _i32p, _i32p, _dp,
+                                             ctypes.c_size_t, _i64p, _i32p, _i32p, _dp]
+        L.sbdgpu_genop_mult.argtypes = [_vp, _dp, _dp]
+        L.sbdgpu_genop_mult_device.argtypes = [_vp, _vp, _vp]
+        L.sbdgpu_genop_diagonal.argtypes = [_vp, _dp]
+        L.sbdgpu_genop_lanczos.argtypes = [_vp, _dp, ctypes.c_int, ctypes.c_double, _dp,
+                                           ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_genop_davidson.argtypes = [_vp, ctypes.POINTER(Opts), _dp, _dp, _dp, _dp, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_int)]
+        L.sbdgpu_genop_last_error.restype = ctypes.c_char_p
+        L.sbdgpu_genop_last_error.argtypes = [_vp]
+        L.sbdgpu_genop_destroy.argtypes = [_vp]
         _lib = L
     return _lib
 
@@ -322,3 +339,104 @@ def context_from_integrals(ints, astr, bstr, device: int = 0) -> Context:
     """Context from an object with .norb, .ecore, .h [L,L] and .eri [L,L,L,L]."""
     from .synth import pack_eri
     return Context(ints.norb, astr, bstr, ints.ecore, ints.h, pack_eri(ints.eri), device)
+
+
+class GenOp:
+    """A second-quantised operator on a basis of bit strings on one GPU (the
+    generic path: basic/generalop.h GeneralOp, basic/basis.h Basis,
+    basic/out_of_place_func/mult.h, lanczos.h, davidson.h).
+
+    states: uint64 array [n, nwords] (or [n] for nwords = 1), site q at bit
+    q % 64 of word q // 64; vectors follow its order.  Terms are given per list
+    (diagonal, off-diagonal) as sequences of (coef, ops) or (coef, ops, n_dag),
+    ops a list of (dag, site) in the order written; n_dag defaults to the
+    number of creation operators (ProductOp::n_dag)."""
+
+    def __init__(self, states, sign: bool = True, device: int = 0):
+        st = np.ascontiguousarray(states, dtype=np.uint64)
+        if st.ndim == 1:
+            st = st[:, None]
+        self.n, self.nwords = st.shape
+        self._states = st
+        self._h = _vp()
+        rc = lib().sbdgpu_genop_create(ctypes.byref(self._h), int(device), int(self.nwords), int(self.n),
+                                       _p(st, _u64p), 1 if sign else 0)
+        if rc != 0:
+            self._h = _vp()
+            raise SbdGpuError(f"sbdgpu_genop_create failed with status {rc}")
+
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = lib().sbdgpu_genop_last_error(self._h)
+            raise SbdGpuError(f"status {rc}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self._h:
+            lib().sbdgpu_genop_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _flatten(terms):
+        off, ops, ndag, coef = [0], [], [], []
+        for t in terms:
+            c, fops = t[0], t[1]
+            nd = t[2] if len(t) > 2 else sum(1 for d, _ in fops if d)  # ProductOp::n_dag
+            ops.extend(int(q) | (0x10000 if d else 0) for d, q in fops)
+            off.append(len(ops))
+            ndag.append(int(nd))
+            coef.append(float(c))
+        return (np.asarray(off, dtype=np.int64), np.asarray(ops if ops else [0], dtype=np.int32),
+                np.asarray(ndag if ndag else [0], dtype=np.int32), np.asarray(coef if coef else [0.0]),
+                len(coef))
+
+    def set_terms(self, diag_terms, off_terms):
+        i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+        d = self._flatten(diag_terms)
+        o = self._flatten(off_terms)
+        self._keep = (d, o)
+        self._check(lib().sbdgpu_genop_set_terms(
+            self._h, d[4], _p(d[0], i64p), _p(d[1], i32p), _p(d[2], i32p), _p(d[3], _dp),
+            o[4], _p(o[0], i64p), _p(o[1], i32p), _p(o[2], i32p), _p(o[3], _dp)))
+
+    def mult(self, C: np.ndarray, W: np.ndarray | None = None) -> np.ndarray:
+        """W + H C (W = 0 when not given)."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        out = np.zeros(self.n) if W is None else np.array(W, dtype=np.float64)
+        self._check(lib().sbdgpu_genop_mult(self._h, _p(C, _dp), _p(out, _dp)))
+        return out
+
+    def mult_device(self, dC_ptr: int, dW_ptr: int) -> None:
+        self._check(lib().sbdgpu_genop_mult_device(self._h, _vp(dC_ptr), _vp(dW_ptr)))
+
+    def diagonal(self) -> np.ndarray:
+        out = np.empty(self.n)
+        self._check(lib().sbdgpu_genop_diagonal(self._h, _p(out, _dp)))
+        return out
+
+    def lanczos(self, W0: np.ndarray, max_it: int, eps: float):
+        """(energy, Ritz vector, Lanczos steps)."""
+        W = np.array(W0, dtype=np.float64)
+        e = ctypes.c_double(0.0)
+        it = ctypes.c_int(0)
+        self._check(lib().sbdgpu_genop_lanczos(self._h, _p(W, _dp), int(max_it), float(eps), ctypes.byref(e),
+                                               ctypes.byref(it)))
+        return e.value, W, it.value
+
+    def davidson(self, W0: np.ndarray, max_it: int, max_nb: int, eps: float, verbose: bool = False):
+        """(energy <W|HW>, W, energy trace, residual trace)."""
+        o = Opts(max_it, max_nb, eps, 86400.0, FP64, 1 if verbose else 0, 0, 0, PRECOND_DIAGONAL)
+        W = np.array(W0, dtype=np.float64)
+        cap = max_it * max_nb
+        te, tt = np.zeros(cap), np.zeros(cap)
+        e = ctypes.c_double(0.0)
+        steps = ctypes.c_int(0)
+        self._check(lib().sbdgpu_genop_davidson(self._h, ctypes.byref(o), _p(W, _dp), ctypes.byref(e), _p(te, _dp),
+                                                _p(tt, _dp), cap, ctypes.byref(steps)))
+        k = min(steps.value, cap)
+        return e.value, W, te[:k], tt[:k]

@@ -255,6 +255,7 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
   // residual falling; the diagonal one otherwise
   bool use_learned = o->precond == SBDGPU_PRECOND_LEARNED && sbdgpu::learned_ready(c);
   double tol_learned_cycle = 1e300;
+  double tol_thick_cycle = 1e300;
   auto add_correction = [&](int into, double e0) {
     if (use_learned)
       sbdgpu::learned_precondition(c, R, e0, eps_reg, X);
@@ -323,9 +324,18 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
           break;
         }
       }
+      // the kept vectors' sigma are FP32 linear combinations carried from cycle
+      // to cycle, so their rounding accumulates; a thick-restart cycle that cut
+      // the residual norm by less than 10 % restarts from the Ritz vector alone
+      // (its sigma computed afresh) instead
+      bool drifted = false;
+      if (ib == nb - 1 && keep > 1) {
+        drifted = tol > 0.9 * tol_thick_cycle;
+        tol_thick_cycle = drifted ? 1e300 : tol;
+      }
       if (ib < nb - 1) {
         add_correction(ib + 1, E[0]);
-      } else if (keep > 1) {
+      } else if (keep > 1 && !drifted) {
         // thick restart: the keep_ritz lowest Ritz vectors (and the previous
         // step's Ritz vector, orthonormalised against them in the small space)
         // with their sigma vectors, as linear combinations of the basis

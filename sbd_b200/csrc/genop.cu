@@ -1,0 +1,677 @@
+// The generic path: a second-quantised operator (basic/generalop.h GeneralOp)
+// applied to a vector on a basis of bit strings (basic/basis.h Basis), and the
+// Lanczos and Davidson solvers built on it (basic/out_of_place_func/mult.h,
+// lanczos.h, davidson.h), at one rank on one GPU.
+//
+// Layout in HBM:
+//   states      [n][nw] uint64 in the caller's order (site q at bit q%64 of
+//               word q/64), nw = 1, 2 or 4
+//   keys, perm  the states sorted (most significant word first) and, per
+//               sorted position, the caller's index: the target of every
+//               off-diagonal term is found by a branch-free binary search
+//   terms       the off-diagonal list as fixed-size records: annihilation and
+//               creation masks (the sites of the first n_dag operators and of
+//               the rest), the coefficient and the operator sites in order
+//               (for the fermionic sign); the diagonal list is folded into one
+//               number per state at set-up (hdiag)
+//
+// mult: one thread per bra state, the term records staged through shared
+// memory in chunks that every warp reads as broadcasts; a term applies when
+// its annihilated sites are occupied and its created sites empty after the
+// annihilation (two mask tests per word), which is the reference's sequential
+// test (mult.h:213-240) for terms whose annihilated sites are distinct and
+// whose created sites are distinct (a term that repeats a site in either part
+// never applies there and is dropped at set-up).  Each thread accumulates its
+// own W_i, so no atomics.  The work is integer and bound by the binary
+// searches' L2 reads, not by HBM.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <iostream>
+#include <numeric>
+
+#include "internal.cuh"
+
+using sbdgpu::Error;
+
+struct sbdgpu_genop {
+  sbdgpu_ctx base;  // device, stream, reduction scratch and the error string
+  int nw = 1;
+  size_t n = 0;
+  int sign = 1;
+  uint64_t* states = nullptr;
+  uint64_t* keys = nullptr;
+  int64_t* perm = nullptr;
+  void* terms = nullptr;       // off-diagonal records
+  size_t n_terms = 0;
+  void* self_terms = nullptr;  // off-diagonal records that map a state onto itself
+  size_t n_self = 0;
+  double* hdiag = nullptr;     // diagonal list, per state (caller order)
+  bool ready = false;
+};
+
+namespace {
+
+constexpr int kMaxOps = SBDGPU_GENOP_MAX_OPS;
+constexpr int kThreads = 256;
+constexpr int kChunk = 128;  // term records per shared-memory chunk
+
+template <int NW>
+struct Term {
+  uint64_t ann[NW];
+  uint64_t cre[NW];
+  double coef;
+  int32_t nops, ndag;
+  uint8_t site[kMaxOps];
+};
+
+template <int NW>
+struct DiagTerm {
+  uint64_t mask[NW];
+  double coef;
+};
+
+template <int NW>
+__device__ __forceinline__ bool key_less(const uint64_t* a, const uint64_t* b) {
+#pragma unroll
+  for (int w = NW - 1; w >= 0; w--)
+    if (a[w] != b[w]) return a[w] < b[w];
+  return false;
+}
+
+// sorted position of w, or -1
+template <int NW>
+__device__ __forceinline__ int64_t find_state(const uint64_t* __restrict__ keys, size_t n, const uint64_t* w) {
+  size_t lo = 0, len = n;
+  while (len > 0) {  // lower bound
+    size_t half = len >> 1;
+    uint64_t k[NW];
+#pragma unroll
+    for (int x = 0; x < NW; x++) k[x] = __ldg(&keys[(lo + half) * NW + x]);
+    if (key_less<NW>(k, w)) {
+      lo += half + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  if (lo >= n) return -1;
+#pragma unroll
+  for (int x = 0; x < NW; x++)
+    if (__ldg(&keys[lo * NW + x]) != w[x]) return -1;
+  return (int64_t)lo;
+}
+
+// parity of the occupied sites below q
+template <int NW>
+__device__ __forceinline__ int parity_below(const uint64_t* w, int q) {
+  int c = 0;
+  const int r = q >> 6;
+#pragma unroll
+  for (int x = 0; x < NW; x++) {
+    if (x < r) c += __popcll(w[x]);
+    else if (x == r) c += __popcll(w[x] & ((1ull << (q & 63)) - 1ull));
+  }
+  return c & 1;
+}
+
+// Apply term t to state v: false when it does not apply; else the target in
+// w and the sign (+1 or -1; +1 when sign is off).
+template <int NW>
+__device__ __forceinline__ bool apply_term(const Term<NW>& t, const uint64_t* v, int sign, uint64_t* w, double* s) {
+  bool ok = true;
+#pragma unroll
+  for (int x = 0; x < NW; x++) {
+    ok &= (v[x] & t.ann[x]) == t.ann[x];
+    ok &= ((v[x] & ~t.ann[x]) & t.cre[x]) == 0ull;
+  }
+  if (!ok) return false;
+  int par = 0;
+  if (sign) {
+#pragma unroll
+    for (int x = 0; x < NW; x++) w[x] = v[x];
+    for (int k = 0; k < t.nops; k++) {
+      const int q = t.site[k];
+      const uint64_t b = 1ull << (q & 63);
+      if (k < t.ndag) w[q >> 6] &= ~b;
+      else w[q >> 6] |= b;
+      par ^= parity_below<NW>(w, q);
+    }
+  } else {
+#pragma unroll
+    for (int x = 0; x < NW; x++) w[x] = (v[x] & ~t.ann[x]) | t.cre[x];
+  }
+  *s = par ? -1.0 : 1.0;
+  return true;
+}
+
+// W[i] += hdiag[i] C[i] + sum over off-diagonal terms of coef * sign * C[j]
+template <int NW>
+__global__ void __launch_bounds__(kThreads) mult_kernel(const uint64_t* __restrict__ states,
+                                                       const uint64_t* __restrict__ keys,
+                                                       const int64_t* __restrict__ perm, size_t n,
+                                                       const Term<NW>* __restrict__ terms, size_t n_terms, int sign,
+                                                       const double* __restrict__ hdiag,
+                                                       const double* __restrict__ C, double* __restrict__ W) {
+  __shared__ Term<NW> sm[kChunk];
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  const bool live = i < n;
+  uint64_t v[NW];
+  double acc = 0.0;
+  if (live) {
+#pragma unroll
+    for (int x = 0; x < NW; x++) v[x] = states[i * NW + x];
+    acc = W[i] + hdiag[i] * C[i];
+  }
+  for (size_t t0 = 0; t0 < n_terms; t0 += kChunk) {
+    const int cnt = (int)min((size_t)kChunk, n_terms - t0);
+    __syncthreads();
+    {
+      // the chunk as 8-byte words
+      const uint64_t* src = reinterpret_cast<const uint64_t*>(terms + t0);
+      uint64_t* dst = reinterpret_cast<uint64_t*>(sm);
+      const int words = cnt * (int)(sizeof(Term<NW>) / 8);
+      for (int k = threadIdx.x; k < words; k += kThreads) dst[k] = src[k];
+    }
+    __syncthreads();
+    if (!live) continue;
+    for (int k = 0; k < cnt; k++) {
+      uint64_t w[NW];
+      double s;
+      if (!apply_term<NW>(sm[k], v, sign, w, &s)) continue;
+      const int64_t j = find_state<NW>(keys, n, w);
+      if (j >= 0) acc += sm[k].coef * s * __ldg(&C[__ldg(&perm[j])]);
+    }
+  }
+  if (live) W[i] = acc;
+}
+
+// hdiag[i] = sum of the diagonal terms whose sites are all occupied in state i
+template <int NW>
+__global__ void __launch_bounds__(kThreads) diag_kernel(const uint64_t* __restrict__ states, size_t n,
+                                                       const DiagTerm<NW>* __restrict__ terms, size_t n_terms,
+                                                       double* __restrict__ hdiag) {
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  uint64_t v[NW];
+#pragma unroll
+  for (int x = 0; x < NW; x++) v[x] = states[i * NW + x];
+  double acc = 0.0;
+  for (size_t k = 0; k < n_terms; k++) {
+    bool ok = true;
+#pragma unroll
+    for (int x = 0; x < NW; x++) ok &= (v[x] & terms[k].mask[x]) == terms[k].mask[x];
+    if (ok) acc += terms[k].coef;
+  }
+  hdiag[i] = acc;
+}
+
+// out[i] = hdiag[i] + sum of the self-mapping off-diagonal terms that apply
+template <int NW>
+__global__ void __launch_bounds__(kThreads) self_kernel(const uint64_t* __restrict__ states, size_t n,
+                                                       const Term<NW>* __restrict__ terms, size_t n_terms, int sign,
+                                                       const double* __restrict__ hdiag, double* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  uint64_t v[NW];
+#pragma unroll
+  for (int x = 0; x < NW; x++) v[x] = states[i * NW + x];
+  double acc = hdiag[i];
+  for (size_t k = 0; k < n_terms; k++) {
+    uint64_t w[NW];
+    double s;
+    if (apply_term<NW>(terms[k], v, sign, w, &s)) acc += terms[k].coef * s;
+  }
+  out[i] = acc;
+}
+
+unsigned blocks_for(size_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+
+template <class F>
+int guarded(sbdgpu_genop* g, F&& f) {
+  if (!g) return SBDGPU_ERR_ARG;
+  try {
+    cudaError_t e = cudaSetDevice(g->base.device);
+    if (e != cudaSuccess) throw Error{SBDGPU_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e)};
+    f();
+    g->base.err.clear();
+    return SBDGPU_OK;
+  } catch (const Error& e) {
+    g->base.err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g->base.err = "host allocation failed";
+    return SBDGPU_ERR_ALLOC;
+  } catch (const std::exception& e) {
+    g->base.err = e.what();
+    return SBDGPU_ERR_STATE;
+  }
+}
+
+// One list's terms as host records.  Off-diagonal terms that repeat a site
+// among their annihilated or among their created operators never apply
+// (the reference's sequential test fails at the repeat) and are left out.
+template <int NW>
+void build_terms(int nw, size_t n_terms, const int64_t* off, const int32_t* ops, const int32_t* ndag,
+                 const double* coef, std::vector<Term<NW>>& all, std::vector<Term<NW>>& self) {
+  const int max_site = 64 * nw;
+  for (size_t k = 0; k < n_terms; k++) {
+    const int64_t a = off[k], b = off[k + 1];
+    if (b < a) throw Error{SBDGPU_ERR_ARG, "term offsets must not decrease"};
+    const int nops = (int)(b - a);
+    if (nops > kMaxOps) throw Error{SBDGPU_ERR_ARG, "more than " + std::to_string(kMaxOps) + " operators in a term"};
+    if (ndag[k] < 0 || ndag[k] > nops) throw Error{SBDGPU_ERR_ARG, "n_dag out of range"};
+    Term<NW> t;
+    std::memset(&t, 0, sizeof(t));
+    t.coef = coef[k];
+    t.nops = nops;
+    t.ndag = ndag[k];
+    bool repeat = false;
+    for (int j = 0; j < nops; j++) {
+      const int q = ops[a + j] & 0xFFFF;
+      if (q >= max_site) throw Error{SBDGPU_ERR_ARG, "site " + std::to_string(q) + " beyond the state width"};
+      t.site[j] = (uint8_t)q;
+      uint64_t* m = j < t.ndag ? t.ann : t.cre;
+      const uint64_t bit = 1ull << (q & 63);
+      if (m[q >> 6] & bit) repeat = true;
+      m[q >> 6] |= bit;
+    }
+    if (repeat) continue;
+    all.push_back(t);
+    if (std::equal(t.ann, t.ann + NW, t.cre)) self.push_back(t);
+  }
+}
+
+template <int NW>
+void set_terms_nw(sbdgpu_genop* g, size_t n_diag, const int64_t* diag_off, const int32_t* diag_ops,
+                  const int32_t* diag_ndag, const double* diag_coef, size_t n_off, const int64_t* off_off,
+                  const int32_t* off_ops, const int32_t* off_ndag, const double* off_coef) {
+  cudaStream_t st = g->base.stream;
+  std::vector<DiagTerm<NW>> dt;
+  dt.reserve(n_diag);
+  for (size_t k = 0; k < n_diag; k++) {
+    const int64_t a = diag_off[k], b = diag_off[k + 1];
+    if (b < a) throw Error{SBDGPU_ERR_ARG, "term offsets must not decrease"};
+    if (diag_ndag[k] < 0 || diag_ndag[k] > b - a) throw Error{SBDGPU_ERR_ARG, "n_dag out of range"};
+    DiagTerm<NW> d;
+    std::memset(&d, 0, sizeof(d));
+    d.coef = diag_coef[k];
+    for (int j = 0; j < diag_ndag[k]; j++) {  // the sites of the first n_dag operators (mult.h:130-139)
+      const int q = diag_ops[a + j] & 0xFFFF;
+      if (q >= 64 * NW) throw Error{SBDGPU_ERR_ARG, "site " + std::to_string(q) + " beyond the state width"};
+      d.mask[q >> 6] |= 1ull << (q & 63);
+    }
+    dt.push_back(d);
+  }
+  std::vector<Term<NW>> all, self;
+  build_terms<NW>(NW, n_off, off_off, off_ops, off_ndag, off_coef, all, self);
+  cudaFree(g->terms);
+  cudaFree(g->self_terms);
+  g->terms = g->self_terms = nullptr;
+  g->ready = false;
+  DiagTerm<NW>* d_dt = nullptr;
+  try {
+    if (!dt.empty()) {
+      d_dt = (DiagTerm<NW>*)sbdgpu::dev_alloc(sizeof(DiagTerm<NW>) * dt.size());
+      SBD_CUDA(cudaMemcpyAsync(d_dt, dt.data(), sizeof(DiagTerm<NW>) * dt.size(), cudaMemcpyHostToDevice, st));
+    }
+    if (!g->hdiag) g->hdiag = (double*)sbdgpu::dev_alloc(sizeof(double) * g->n);
+    diag_kernel<NW><<<blocks_for(g->n), kThreads, 0, st>>>(g->states, g->n, d_dt, dt.size(), g->hdiag);
+    SBD_CUDA(cudaGetLastError());
+    if (!all.empty()) {
+      g->terms = sbdgpu::dev_alloc(sizeof(Term<NW>) * all.size());
+      SBD_CUDA(cudaMemcpyAsync(g->terms, all.data(), sizeof(Term<NW>) * all.size(), cudaMemcpyHostToDevice, st));
+    }
+    if (!self.empty()) {
+      g->self_terms = sbdgpu::dev_alloc(sizeof(Term<NW>) * self.size());
+      SBD_CUDA(cudaMemcpyAsync(g->self_terms, self.data(), sizeof(Term<NW>) * self.size(), cudaMemcpyHostToDevice,
+                               st));
+    }
+    SBD_CUDA(cudaStreamSynchronize(st));
+  } catch (...) {
+    cudaFree(d_dt);
+    throw;
+  }
+  cudaFree(d_dt);
+  g->n_terms = all.size();
+  g->n_self = self.size();
+  g->ready = true;
+}
+
+template <int NW>
+void mult_nw(sbdgpu_genop* g, const double* C, double* W) {
+  mult_kernel<NW><<<blocks_for(g->n), kThreads, 0, g->base.stream>>>(
+      g->states, g->keys, g->perm, g->n, static_cast<const Term<NW>*>(g->terms), g->n_terms, g->sign, g->hdiag, C, W);
+  SBD_CUDA(cudaGetLastError());
+}
+
+void mult(sbdgpu_genop* g, const double* C, double* W) {
+  if (!g->ready) throw Error{SBDGPU_ERR_STATE, "no operator: call sbdgpu_genop_set_terms first"};
+  switch (g->nw) {
+    case 1: mult_nw<1>(g, C, W); break;
+    case 2: mult_nw<2>(g, C, W); break;
+    default: mult_nw<4>(g, C, W); break;
+  }
+}
+
+void diagonal(sbdgpu_genop* g, double* out) {
+  if (!g->ready) throw Error{SBDGPU_ERR_STATE, "no operator: call sbdgpu_genop_set_terms first"};
+  cudaStream_t st = g->base.stream;
+  switch (g->nw) {
+    case 1:
+      self_kernel<1><<<blocks_for(g->n), kThreads, 0, st>>>(g->states, g->n, static_cast<const Term<1>*>(g->self_terms),
+                                                            g->n_self, g->sign, g->hdiag, out);
+      break;
+    case 2:
+      self_kernel<2><<<blocks_for(g->n), kThreads, 0, st>>>(g->states, g->n, static_cast<const Term<2>*>(g->self_terms),
+                                                            g->n_self, g->sign, g->hdiag, out);
+      break;
+    default:
+      self_kernel<4><<<blocks_for(g->n), kThreads, 0, st>>>(g->states, g->n, static_cast<const Term<4>*>(g->self_terms),
+                                                            g->n_self, g->sign, g->hdiag, out);
+      break;
+  }
+  SBD_CUDA(cudaGetLastError());
+}
+
+struct DevVecs {
+  std::vector<double*> p;
+  cudaStream_t s;
+  ~DevVecs() {
+    cudaStreamSynchronize(s);
+    for (auto x : p) cudaFree(x);
+  }
+  double* add(size_t n) {
+    p.push_back((double*)sbdgpu::dev_alloc(sizeof(double) * n));
+    return p.back();
+  }
+};
+
+// swap of framework/dm_vector.h:89-101: X <- b Y, Y <- a X
+__global__ void swap_kernel(double a, double* __restrict__ X, double b, double* __restrict__ Y, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double c = a * X[i];
+    X[i] = b * Y[i];
+    Y[i] = c;
+  }
+}
+
+void lanczos(sbdgpu_genop* g, double* Wh, int max_it, double eps, double* energy, int* n_iter) {
+  if (max_it < 1) throw Error{SBDGPU_ERR_ARG, "max_it must be positive"};
+  const size_t n = g->n;
+  cudaStream_t st = g->base.stream;
+  sbdgpu_ctx* c = &g->base;
+  DevVecs v{{}, st};
+  double* W = v.add(n);
+  double* C0 = v.add(n);
+  double* C1 = v.add(n);
+  SBD_CUDA(cudaMemcpyAsync(W, Wh, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  SBD_CUDA(cudaMemcpyAsync(C0, W, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  SBD_CUDA(cudaMemsetAsync(C1, 0, sizeof(double) * n, st));
+  const int lda = max_it;
+  std::vector<double> A((size_t)lda * lda, 0.0), U((size_t)lda * lda, 0.0), E(lda, 0.0);
+  double e_old = 1.0e8;
+  int it_stop = 0, steps = 0;
+  const unsigned nblk = std::min<size_t>(blocks_for(n), 148 * 8);
+  for (int it = 0; it < max_it; it++) {
+    steps++;
+    const int ii = it + lda * it, ij = it + lda * (it + 1), ji = it + 1 + lda * it;
+    mult(g, C0, C1);
+    const double aii = sbdgpu::dot(c, C0, C1, n);
+    A[ii] = aii;
+    for (int i = 0; i < steps; i++)
+      for (int j = 0; j < steps; j++) U[i + lda * j] = A[i + lda * j];
+    sbdgpu::jacobi_eig(steps, U.data(), lda, E.data());
+    if (std::abs(E[0] - e_old) < eps || it + 1 == max_it) {
+      it_stop = it;
+      break;
+    }
+    e_old = E[0];
+    sbdgpu::axpy(C1, C0, -aii, n, st);
+    const double b = std::sqrt(sbdgpu::dot(c, C1, C1, n));
+    sbdgpu::scale(C1, 1.0 / b, n, st);
+    A[ij] = A[ji] = b;
+    if (std::abs(b) < eps) {
+      it_stop = it;
+      break;
+    }
+    swap_kernel<<<nblk, kThreads, 0, st>>>(-b, C0, 1.0, C1, n);
+    SBD_CUDA(cudaGetLastError());
+  }
+  // the Ritz vector from a second pass of the recurrence (lanczos.h:276-302)
+  SBD_CUDA(cudaMemcpyAsync(C0, W, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  SBD_CUDA(cudaMemsetAsync(C1, 0, sizeof(double) * n, st));
+  sbdgpu::scale(W, U[0], n, st);
+  for (int it = 0; it < it_stop; it++) {
+    const int ii = it + lda * it;
+    mult(g, C0, C1);
+    sbdgpu::axpy(C1, C0, -A[ii], n, st);
+    const double b = std::sqrt(sbdgpu::dot(c, C1, C1, n));
+    sbdgpu::scale(C1, 1.0 / b, n, st);
+    sbdgpu::axpy(W, C1, U[it + 1], n, st);
+    swap_kernel<<<nblk, kThreads, 0, st>>>(-b, C0, 1.0, C1, n);
+    SBD_CUDA(cudaGetLastError());
+  }
+  SBD_CUDA(cudaMemcpyAsync(Wh, W, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  SBD_CUDA(cudaStreamSynchronize(st));
+  if (energy) *energy = E[0];
+  if (n_iter) *n_iter = steps;
+}
+
+void davidson(sbdgpu_genop* g, const sbdgpu_opts* o, double* Wh, double* energy, double* trace_e, double* trace_tol,
+              int max_trace, int* n_steps) {
+  const int nb = o->max_nb;
+  if (nb < 1 || nb > 32) throw Error{SBDGPU_ERR_ARG, "max_nb must be in [1, 32]"};
+  const size_t n = g->n;
+  cudaStream_t st = g->base.stream;
+  sbdgpu_ctx* c = &g->base;
+  DevVecs v{{}, st};
+  double* W = v.add(n);
+  double* R = v.add(n);
+  double* hii = v.add(n);
+  std::vector<double*> C(nb), HC(nb);
+  for (int k = 0; k < nb; k++) {
+    C[k] = v.add(n);
+    HC[k] = v.add(n);
+  }
+  diagonal(g, hii);
+  SBD_CUDA(cudaMemcpyAsync(W, Wh, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  const double eps_reg = 1.0e-12;
+  std::vector<double> H(nb * nb, 0.0), U(nb * nb, 0.0), E(nb, 0.0);
+  int steps = 0;
+  bool cont = true;
+  for (int it = 0; it < o->max_it && cont; it++) {
+    SBD_CUDA(cudaMemcpyAsync(C[0], W, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    for (int ib = 0; ib < nb; ib++) {
+      SBD_CUDA(cudaMemsetAsync(HC[ib], 0, sizeof(double) * n, st));
+      mult(g, C[ib], HC[ib]);
+      for (int jb = 0; jb <= ib; jb++) {
+        H[jb + nb * ib] = sbdgpu::dot(c, C[jb], HC[ib], n);
+        H[ib + nb * jb] = H[jb + nb * ib];
+      }
+      for (int jb = 0; jb <= ib; jb++)
+        for (int kb = 0; kb <= ib; kb++) U[jb + nb * kb] = H[jb + nb * kb];
+      sbdgpu::jacobi_eig(ib + 1, U.data(), nb, E.data());
+      sbdgpu::ritz_update(C.data(), HC.data(), U.data(), ib + 1, E[0], W, R, n, st);
+      const double nw = std::sqrt(sbdgpu::dot(c, W, W, n));
+      sbdgpu::scale(W, 1.0 / nw, n, st);
+      const double tol = std::sqrt(sbdgpu::dot(c, R, R, n));
+      sbdgpu::scale(R, 1.0 / tol, n, st);
+      if (trace_e && steps < max_trace) trace_e[steps] = E[0];
+      if (trace_tol && steps < max_trace) trace_tol[steps] = tol;
+      steps++;
+      if (o->verbose) {
+        std::cout << " Davidson iteration " << it << "." << ib << " (tol = " << tol << "):";
+        for (int p = 0; p < std::min(ib + 1, 4); p++) std::cout << " " << E[p];
+        std::cout << std::endl;
+      }
+      if (tol < o->eps) {
+        cont = false;
+        break;
+      }
+      if (ib < nb - 1) {
+        sbdgpu::precondition(R, hii, E[0], eps_reg, C[ib + 1], n, st);
+        for (int kb = 0; kb < ib + 1; kb++) {
+          const double olap = sbdgpu::dot(c, C[kb], C[ib + 1], n);
+          sbdgpu::axpy(C[ib + 1], C[kb], -olap, n, st);
+        }
+        const double nc = std::sqrt(sbdgpu::dot(c, C[ib + 1], C[ib + 1], n));
+        sbdgpu::scale(C[ib + 1], 1.0 / nc, n, st);
+      }
+    }
+  }
+  SBD_CUDA(cudaMemsetAsync(R, 0, sizeof(double) * n, st));
+  mult(g, W, R);
+  const double e = sbdgpu::dot(c, W, R, n);
+  SBD_CUDA(cudaMemcpyAsync(Wh, W, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  SBD_CUDA(cudaStreamSynchronize(st));
+  if (energy) *energy = e;
+  if (n_steps) *n_steps = steps;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sbdgpu_genop_create(sbdgpu_genop** out, int device, int nwords, size_t nstates, const uint64_t* states,
+                        int sign) {
+  if (!out) return SBDGPU_ERR_ARG;
+  *out = nullptr;
+  auto* g = new (std::nothrow) sbdgpu_genop();
+  if (!g) return SBDGPU_ERR_ALLOC;
+  g->base.device = device;
+  int rc = guarded(g, [&] {
+    if (nwords != 1 && nwords != 2 && nwords != 4) throw Error{SBDGPU_ERR_ARG, "nwords must be 1, 2 or 4"};
+    if (nstates == 0 || !states) throw Error{SBDGPU_ERR_ARG, "empty basis"};
+    g->nw = nwords;
+    g->n = nstates;
+    g->sign = sign ? 1 : 0;
+    SBD_CUDA(cudaStreamCreateWithFlags(&g->base.stream, cudaStreamNonBlocking));
+    std::vector<int64_t> order(nstates);
+    std::iota(order.begin(), order.end(), 0);
+    auto less = [&](int64_t a, int64_t b) {
+      for (int w = nwords - 1; w >= 0; w--) {
+        const uint64_t x = states[a * nwords + w], y = states[b * nwords + w];
+        if (x != y) return x < y;
+      }
+      return false;
+    };
+    std::sort(order.begin(), order.end(), less);
+    std::vector<uint64_t> keys(nstates * nwords);
+    for (size_t i = 0; i < nstates; i++) {
+      if (i > 0 && !less(order[i - 1], order[i])) throw Error{SBDGPU_ERR_ARG, "repeated basis state"};
+      std::memcpy(&keys[i * nwords], &states[order[i] * nwords], sizeof(uint64_t) * nwords);
+    }
+    const size_t bytes = sizeof(uint64_t) * nstates * nwords;
+    g->states = (uint64_t*)sbdgpu::dev_alloc(bytes);
+    g->keys = (uint64_t*)sbdgpu::dev_alloc(bytes);
+    g->perm = (int64_t*)sbdgpu::dev_alloc(sizeof(int64_t) * nstates);
+    SBD_CUDA(cudaMemcpyAsync(g->states, states, bytes, cudaMemcpyHostToDevice, g->base.stream));
+    SBD_CUDA(cudaMemcpyAsync(g->keys, keys.data(), bytes, cudaMemcpyHostToDevice, g->base.stream));
+    SBD_CUDA(cudaMemcpyAsync(g->perm, order.data(), sizeof(int64_t) * nstates, cudaMemcpyHostToDevice,
+                             g->base.stream));
+    SBD_CUDA(cudaStreamSynchronize(g->base.stream));
+  });
+  if (rc != SBDGPU_OK) {  // a bad argument, or no memory on the device
+    sbdgpu_genop_destroy(g);
+    return rc;
+  }
+  *out = g;
+  return SBDGPU_OK;
+}
+
+int sbdgpu_genop_set_terms(sbdgpu_genop* g, size_t n_diag, const int64_t* diag_off, const int32_t* diag_ops,
+                           const int32_t* diag_ndag, const double* diag_coef, size_t n_off, const int64_t* off_off,
+                           const int32_t* off_ops, const int32_t* off_ndag, const double* off_coef) {
+  return guarded(g, [&] {
+    if ((n_diag && (!diag_off || !diag_ndag || !diag_coef)) || (n_off && (!off_off || !off_ndag || !off_coef)))
+      throw Error{SBDGPU_ERR_ARG, "null term array"};
+    switch (g->nw) {
+      case 1:
+        set_terms_nw<1>(g, n_diag, diag_off, diag_ops, diag_ndag, diag_coef, n_off, off_off, off_ops, off_ndag,
+                        off_coef);
+        break;
+      case 2:
+        set_terms_nw<2>(g, n_diag, diag_off, diag_ops, diag_ndag, diag_coef, n_off, off_off, off_ops, off_ndag,
+                        off_coef);
+        break;
+      default:
+        set_terms_nw<4>(g, n_diag, diag_off, diag_ops, diag_ndag, diag_coef, n_off, off_off, off_ops, off_ndag,
+                        off_coef);
+        break;
+    }
+  });
+}
+
+int sbdgpu_genop_mult_device(sbdgpu_genop* g, const double* dC, double* dW) {
+  return guarded(g, [&] {
+    if (!dC || !dW) throw Error{SBDGPU_ERR_ARG, "null vector"};
+    mult(g, dC, dW);
+  });
+}
+
+int sbdgpu_genop_mult(sbdgpu_genop* g, const double* C, double* W) {
+  return guarded(g, [&] {
+    if (!C || !W) throw Error{SBDGPU_ERR_ARG, "null vector"};
+    cudaStream_t st = g->base.stream;
+    DevVecs v{{}, st};
+    double* dC = v.add(g->n);
+    double* dW = v.add(g->n);
+    SBD_CUDA(cudaMemcpyAsync(dC, C, sizeof(double) * g->n, cudaMemcpyHostToDevice, st));
+    SBD_CUDA(cudaMemcpyAsync(dW, W, sizeof(double) * g->n, cudaMemcpyHostToDevice, st));
+    mult(g, dC, dW);
+    SBD_CUDA(cudaMemcpyAsync(W, dW, sizeof(double) * g->n, cudaMemcpyDeviceToHost, st));
+    SBD_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int sbdgpu_genop_diagonal(sbdgpu_genop* g, double* hii) {
+  return guarded(g, [&] {
+    if (!hii) throw Error{SBDGPU_ERR_ARG, "null vector"};
+    cudaStream_t st = g->base.stream;
+    DevVecs v{{}, st};
+    double* d = v.add(g->n);
+    diagonal(g, d);
+    SBD_CUDA(cudaMemcpyAsync(hii, d, sizeof(double) * g->n, cudaMemcpyDeviceToHost, st));
+    SBD_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int sbdgpu_genop_lanczos(sbdgpu_genop* g, double* W, int max_it, double eps, double* energy, int* n_iter) {
+  return guarded(g, [&] {
+    if (!W) throw Error{SBDGPU_ERR_ARG, "null vector"};
+    if (!g->ready) throw Error{SBDGPU_ERR_STATE, "no operator: call sbdgpu_genop_set_terms first"};
+    lanczos(g, W, max_it, eps, energy, n_iter);
+  });
+}
+
+int sbdgpu_genop_davidson(sbdgpu_genop* g, const sbdgpu_opts* opts, double* W, double* energy, double* trace_e,
+                          double* trace_tol, int max_trace, int* n_steps) {
+  return guarded(g, [&] {
+    if (!opts || !W) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    if (!g->ready) throw Error{SBDGPU_ERR_STATE, "no operator: call sbdgpu_genop_set_terms first"};
+    davidson(g, opts, W, energy, trace_e, trace_tol, max_trace, n_steps);
+  });
+}
+
+const char* sbdgpu_genop_last_error(sbdgpu_genop* g) { return g ? g->base.err.c_str() : "null object"; }
+
+void sbdgpu_genop_destroy(sbdgpu_genop* g) {
+  if (!g) return;
+  cudaSetDevice(g->base.device);
+  if (g->base.stream) cudaStreamSynchronize(g->base.stream);
+  cudaFree(g->states);
+  cudaFree(g->keys);
+  cudaFree(g->perm);
+  cudaFree(g->terms);
+  cudaFree(g->self_terms);
+  cudaFree(g->hdiag);
+  cudaFree(g->base.red);
+  if (g->base.stream) cudaStreamDestroy(g->base.stream);
+  g->base.red = nullptr;
+  g->base.stream = nullptr;
+  delete g;
+}
+
+}  // extern "C"

@@ -19,7 +19,8 @@ def _ensure_built():
     import oracle
     from sbd_b200 import build
     # make builds the reference checker only where the reference checkout is present
-    if not os.path.exists(oracle.ORACLE_SO) or not oracle.reference_available():
+    if (not os.path.exists(oracle.ORACLE_SO) or not oracle.reference_available()
+            or not os.path.exists(oracle.REF_GENERIC_SO)):
         oracle.build()
     if not os.path.exists(build.LIB):
         build.build_lib()
