@@ -385,6 +385,53 @@ def method1_block(args, dev, hbm_peak, peak_kind):
             "note": "12 bytes per stored element (uint32 ket, FP64 value) + row offsets + hii, C, sigma"}
 
 
+def genop_block(args, dev):
+    """The generic second-quantised path (sbdgpu_genop_*): the FCIDUMP
+    Hamiltonian of the 245,025-determinant system (norb 12, 4a/4b, full
+    space) as a GeneralOp on 24 sites, its on-the-fly mult per second, and its
+    Davidson energy against the tensor-product-basis path's."""
+    import os
+    import tempfile
+    import torch
+    import sbd_b200
+    from sbd_b200 import synth
+    ints, ne, strs = synth.make_workload("c0_L12_4e_full", seed=0)
+    L = ints.norb
+    states = np.array([int(a) | (int(b) << L) for a in strs for b in strs], dtype=np.uint64)
+    g = sbd_b200.GenOp(states, sign=True, device=dev)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "FCIDUMP")
+        synth.write_fcidump(p, ints, 2 * ne)
+        g.set_fcidump(p)
+    n = len(states)
+    C = torch.randn(n, dtype=torch.float64, device=f"cuda:{dev}")
+    Wd = torch.zeros_like(C)
+    for _ in range(3):
+        g.mult_device(C.data_ptr(), Wd.data_ptr())
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    ev0.record()
+    for _ in range(reps):
+        g.mult_device(C.data_ptr(), Wd.data_ptr())
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / reps
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    W0 = np.zeros(n)
+    W0[0] = 1.0
+    e_tpb, _, te_tpb, _ = ctx.davidson(W0, 200, 10, 1e-8)
+    t = time.perf_counter()
+    e_gen, _, te, tt = g.davidson(W0, 200, 10, 1e-8)
+    t_gen = time.perf_counter() - t
+    ctx.close()
+    g.close()
+    return {"workload": "c0_L12_4e_full as GeneralOp (24 sites)", "states": n, "mult_ms": ms, "mult_per_s": 1000.0 / ms, "davidson_steps": len(te),
+            "davidson_s": t_gen, "e_generic": e_gen, "e_tpb": e_tpb, "abs_diff": abs(e_gen - e_tpb),
+            "note": "device-timed mult; no reference arm: the reference's generic mult cannot find most basis "
+                    "states (Basis::IndexSearch bisects over the first nwords states only)"}
+
+
 def config4_block(args, dev, learned):
     """The 400M-determinant workload (norb 48, 10a/10b, 20,000 x 20,000
     selected strings): FP64, FP32 and tensor-core sigma builds per second, and
@@ -663,6 +710,8 @@ def run_gpu(args):
         line["method1_stored"] = method1_block(args, dev, hbm_peak, peak_kind)
     if args.roots > 0:
         line["block_roots"] = roots_block(args, dev)
+    if args.genop and world == 1:
+        line["genop"] = genop_block(args, dev)
     if args.rdm:
         line["rdm"] = rdm_block(args, dev)
     if args.config4 and world == 1:
@@ -707,6 +756,7 @@ def main():
     ap.add_argument("--learn-cg", type=int, default=40, help="MINRES steps per harvested correction")
     ap.add_argument("--learn-steps", type=int, default=600, help="Adam steps of the learned preconditioner")
     ap.add_argument("--rdm", action="store_true", help="also time the 1/2-RDMs")
+    ap.add_argument("--genop", action="store_true", help="also time the generic second-quantised path")
     ap.add_argument("--rdm-workload", default="c1_L26_6e_4000", help="workload of the RDM block")
     ap.add_argument("--config4", action="store_true",
                     help="also run the 400M-determinant workload (norb 48, 10a/10b, 20,000 strings)")

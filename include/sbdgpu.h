@@ -311,6 +311,14 @@ int sbdgpu_genop_set_terms(sbdgpu_genop* g, size_t n_diag, const int64_t* diag_o
                            const int32_t* diag_ndag, const double* diag_coef, size_t n_off, const int64_t* off_off,
                            const int32_t* off_ops, const int32_t* off_ndag, const double* off_coef);
 
+/* The quantum-chemistry Hamiltonian of an FCIDUMP file as the operator
+ * (GeneralOp_From_FCIDump, basic/out_of_place_func/stdmodel.h:13-98: alpha
+ * orbital p at site p, beta at site p + norb), in place of
+ * sbdgpu_genop_set_terms; *norb and *nelec from the file's header.  The
+ * integrals are used at full precision (the reference's MpiBcast of the
+ * FCIDUMP re-reads them at six significant digits). */
+int sbdgpu_genop_set_fcidump(sbdgpu_genop* g, const char* path, int* norb, int* nelec);
+
 /* W += H C (mult.h:268-291 at one rank: the diagonal list, then the
  * off-diagonal one).  Host vectors of nstates doubles; the _device form takes
  * device pointers and runs on the object's stream. */

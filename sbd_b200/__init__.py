@@ -31,7 +31,7 @@ EXPORTS = [
     "sbdgpu_precond_train", "sbdgpu_precond_get", "sbdgpu_precond_set", "sbdgpu_precond_apply",
     "sbdgpu_mlp_loss_grad", "sbdgpu_genop_create", "sbdgpu_genop_set_terms", "sbdgpu_genop_mult",
     "sbdgpu_genop_mult_device", "sbdgpu_genop_diagonal", "sbdgpu_genop_lanczos", "sbdgpu_genop_davidson",
-    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy",
+    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy", "sbdgpu_genop_set_fcidump",
 ]
 
 PRECOND_DIAGONAL = 0
@@ -104,6 +104,8 @@ def lib():
                                           ctypes.c_int]
         L.sbdgpu_genop_set_terms.argtypes = [_vp, ctypes.c_size_t, _i64p, _i32p, _i32p, _dp,
                                              ctypes.c_size_t, _i64p, _i32p, _i32p, _dp]
+        L.sbdgpu_genop_set_fcidump.argtypes = [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_genop_mult.argtypes = [_vp, _dp, _dp]
         L.sbdgpu_genop_mult_device.argtypes = [_vp, _vp, _vp]
         L.sbdgpu_genop_diagonal.argtypes = [_vp, _dp]
@@ -403,6 +405,12 @@ class GenOp:
         self._check(lib().sbdgpu_genop_set_terms(
             self._h, d[4], _p(d[0], i64p), _p(d[1], i32p), _p(d[2], i32p), _p(d[3], _dp),
             o[4], _p(o[0], i64p), _p(o[1], i32p), _p(o[2], i32p), _p(o[3], _dp)))
+
+    def set_fcidump(self, path: str):
+        """The FCIDUMP Hamiltonian as the operator; returns (norb, nelec)."""
+        L, N = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().sbdgpu_genop_set_fcidump(self._h, path.encode(), ctypes.byref(L), ctypes.byref(N)))
+        return L.value, N.value
 
     def mult(self, C: np.ndarray, W: np.ndarray | None = None) -> np.ndarray:
         """W + H C (W = 0 when not given)."""

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsbdgpu.so")
-SOURCES = ["api.cu", "tables.cu", "sigma.cu", "misc.cu", "tc_ab.cu", "noalloc.cu", "stored.cu", "roots.cu", "batch.cu", "learned.cu", "gemm_same.cu", "genop.cu"]
+SOURCES = ["api.cu", "tables.cu", "sigma.cu", "misc.cu", "tc_ab.cu", "noalloc.cu", "stored.cu", "roots.cu", "batch.cu", "learned.cu", "gemm_same.cu", "genop.cu", "genop_fcidump.cu", "rdm.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,7 +30,8 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 def build_lib(force: bool = False, verbose: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, "internal.cuh"), os.path.join(ROOT, "include", "sbdgpu.h")]
+    deps = srcs + [os.path.join(CSRC, "internal.cuh"), os.path.join(ROOT, "include", "sbdgpu.h"),
+                   os.path.join(HERE, "include", "sbd_gpu", "generalop.h"), os.path.join(HERE, "include", "sbd_gpu", "tpb.h")]
     if not force and not _stale(LIB, deps):
         return LIB
     objdir = os.path.join(HERE, "_build")
@@ -40,7 +41,7 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", "g++",
-               "-I", os.path.join(ROOT, "include"), "-c", s, "-o", o]
+               "-I", os.path.join(ROOT, "include"), "-I", os.path.join(HERE, "include"), "-c", s, "-o", o]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append(subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True))

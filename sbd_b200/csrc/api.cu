@@ -765,6 +765,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   sbdgpu::release_hamiltonian(c);
   sbdgpu::free_learned(c);
   sbdgpu::free_dense_same(c);
+  sbdgpu::free_rdm_tables(c);
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);

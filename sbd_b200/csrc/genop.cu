@@ -532,6 +532,10 @@ void davidson(sbdgpu_genop* g, const sbdgpu_opts* o, double* Wh, double* energy,
 
 }  // namespace
 
+namespace sbdgpu {
+void genop_set_error(sbdgpu_genop* g, const std::string& msg) { g->base.err = msg; }
+}  // namespace sbdgpu
+
 extern "C" {
 
 int sbdgpu_genop_create(sbdgpu_genop** out, int device, int nwords, size_t nstates, const uint64_t* states,

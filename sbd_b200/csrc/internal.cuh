@@ -104,6 +104,10 @@ struct sbdgpu_ctx {
   int blk_max = 0;
   size_t blk_r0 = 0, blk_r1 = 0;
   sbdgpu::SpinTables tab[2];
+  // RDM tables: beta singles grouped by excitation, bra row of every alpha single
+  int64_t* rdm_bin_off = nullptr;
+  uint32_t* rdm_bin_ent = nullptr;
+  int32_t* rdm_a_row = nullptr;
   // stored Hamiltonian (method 1): off-diagonal elements, CSR by bra determinant
   int64_t* hs_row = nullptr;   // [N+1]
   uint32_t* hs_col = nullptr;  // ket determinant ja*nb + jb
@@ -157,6 +161,12 @@ void ritz_update(double* const* C, double* const* HC, const double* U, int nk, d
 void precondition(const double* R, const double* hii, double e0, double eps_reg, double* out, size_t n,
                   cudaStream_t s);
 void rdm(sbdgpu_ctx* c, const double* dW, double* one, double* two);
+// rdm.cu: the off-diagonal terms, added into device arrays one [2][L*L] and two [4][L^4]
+void rdm_offdiag(sbdgpu_ctx* c, const double* dW, double* one, double* two);
+void ensure_rdm_tables(sbdgpu_ctx* c);
+void free_rdm_tables(sbdgpu_ctx* c);
+// genop.cu: record an error message on a generic-path object
+void genop_set_error(sbdgpu_genop* g, const std::string& msg);
 void occupation(sbdgpu_ctx* c, const double* dW, double* dens);
 void alpha_weights(sbdgpu_ctx* c, const double* dW, double* D);
 

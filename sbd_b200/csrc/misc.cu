@@ -233,146 +233,6 @@ __global__ void precond_kernel(const double* __restrict__ R, const double* __res
 
 // ---------------------------------------------------------------- RDMs
 
-struct Det {
-  uint64_t lo, hi;  // interleaved spin orbitals 0..63 and 64..127
-};
-
-__device__ __forceinline__ uint64_t spread32(uint64_t x) {
-  x &= 0xFFFFFFFFull;
-  x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
-  x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
-  x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
-  x = (x | (x << 2)) & 0x3333333333333333ull;
-  x = (x | (x << 1)) & 0x5555555555555555ull;
-  return x;
-}
-
-// DetFromAlphaBeta, chemistry/basic/determinants.h:98-119
-__device__ __forceinline__ Det interleave(uint64_t a, uint64_t b) {
-  Det d;
-  d.lo = spread32(a) | (spread32(b) << 1);
-  d.hi = spread32(a >> 32) | (spread32(b >> 32) << 1);
-  return d;
-}
-
-__device__ __forceinline__ uint64_t low_mask(int k) {  // bits [0,k) of a 64-bit word, k in [0,64]
-  return k >= 64 ? ~0ull : ((1ull << k) - 1ull);
-}
-
-// occupied spin orbitals strictly between x and y
-__device__ __forceinline__ double parity(const Det& d, int x, int y) {
-  int lo = x < y ? x : y, hi = x < y ? y : x;
-  int cnt = 0;
-  if (hi - lo >= 2) {
-    int a = lo + 1, b = hi;  // [a, b)
-    uint64_t mlo = low_mask(b < 64 ? b : 64) & ~low_mask(a < 64 ? a : 64);
-    uint64_t mhi = low_mask(b > 64 ? b - 64 : 0) & ~low_mask(a > 64 ? a - 64 : 0);
-    cnt = __popcll(d.lo & mlo) + __popcll(d.hi & mhi);
-  }
-  return (cnt & 1) ? -1.0 : 1.0;
-}
-
-// OneDiffCorrelation, chemistry/tpb/correlation.h:49-86 (det = bra, i created, a annihilated)
-__device__ void one_diff(const Det& det, double v0, int i, int a, int L, double* one, double* two) {
-  size_t L2 = (size_t)L * L, L3 = L2 * L, L4 = L3 * L;
-  double v = v0 * parity(det, i, a);
-  int oi = i / 2, si = i % 2, oa = a / 2;
-  atomicAdd(&one[si * L2 + oi + (size_t)L * oa], v);
-  for (int w = 0; w < 2; w++) {
-    uint64_t bits = w ? det.hi : det.lo;
-    while (bits) {
-      int soj = (__ffsll((long long)bits) - 1) + 64 * w;
-      bits &= bits - 1;
-      int oj = soj / 2, sj = soj % 2;
-      atomicAdd(&two[(si + 2 * sj) * L4 + oa + oj * L + oi * L2 + oj * L3], v);
-      atomicAdd(&two[(sj + 2 * si) * L4 + oj + oa * L + oj * L2 + oi * L3], v);
-      if (si == sj) {
-        atomicAdd(&two[(si + 2 * sj) * L4 + oa + oj * L + oj * L2 + oi * L3], -v);
-        atomicAdd(&two[(sj + 2 * si) * L4 + oj + oa * L + oi * L2 + oj * L3], -v);
-      }
-    }
-  }
-}
-
-// TwoDiffCorrelation, chemistry/tpb/correlation.h:91-130
-__device__ void two_diff(const Det& det, double v0, int i, int j, int a, int b, int L, double* two) {
-  size_t L2 = (size_t)L * L, L4 = L2 * L2;
-  int I = i < j ? i : j, J = i < j ? j : i, A = a < b ? a : b, B = a < b ? b : a;
-  double sgn = parity(det, I, A) * parity(det, J, B);
-  if (A > J || B < I) sgn = -sgn;
-  int oi = I / 2, si = I % 2, oa = A / 2, sa = A % 2, oj = J / 2, sj = J % 2, ob = B / 2, sb = B % 2;
-  double v = sgn * v0;
-  if (si == sa) {
-    atomicAdd(&two[(si + 2 * sj) * L4 + oa + L * ob + L2 * (oi + (size_t)L * oj)], v);
-    atomicAdd(&two[(sj + 2 * si) * L4 + ob + L * oa + L2 * (oj + (size_t)L * oi)], v);
-  }
-  if (si == sb) {
-    atomicAdd(&two[(si + 2 * sj) * L4 + oa + L * ob + L2 * (oj + (size_t)L * oi)], -v);
-    atomicAdd(&two[(sj + 2 * si) * L4 + ob + L * oa + L2 * (oi + (size_t)L * oj)], -v);
-  }
-}
-
-__device__ __forceinline__ int take_bits(const Det& m, int* out) {
-  int n = 0;
-  uint64_t x = m.lo;
-  while (x && n < 3) {
-    out[n++] = __ffsll((long long)x) - 1;
-    x &= x - 1;
-  }
-  x = m.hi;
-  while (x && n < 3) {
-    out[n++] = 64 + __ffsll((long long)x) - 1;
-    x &= x - 1;
-  }
-  return n;
-}
-
-// CorrelationTermAddition, chemistry/tpb/correlation.h:135-189 (off-diagonal kinds)
-__device__ void term(const Det& bra, const Det& ket, double v0, int L, double* one, double* two) {
-  Det cm{bra.lo & ~ket.lo, bra.hi & ~ket.hi}, dm{ket.lo & ~bra.lo, ket.hi & ~bra.hi};
-  int c[3], d[3];
-  int nc = take_bits(cm, c);
-  take_bits(dm, d);
-  if (nc == 1)
-    one_diff(bra, v0, c[0], d[0], L, one, two);
-  else if (nc == 2)
-    two_diff(bra, v0, c[0], c[1], d[0], d[1], L, two);
-}
-
-__global__ void rdm_kernel(const uint64_t* __restrict__ astr, const uint64_t* __restrict__ bstr, size_t na,
-                           size_t nb, int L, const double* __restrict__ W, SpinTables ta, SpinTables tb,
-                           double* one, double* two) {
-  size_t ia = blockIdx.x;
-  size_t ib = (size_t)blockIdx.y * blockDim.x + threadIdx.x;
-  if (ib >= nb) return;
-  double wi = W[ia * nb + ib];
-  if (wi == 0.0) return;
-  Det bra = interleave(astr[ia], bstr[ib]);
-  for (int kind = 0; kind < 2; kind++) {
-    const int64_t* off = kind ? ta.d_off : ta.s_off;
-    const int32_t* idx = kind ? ta.d_idx : ta.s_idx;
-    for (int64_t k = off[ia]; k < off[ia + 1]; k++) {
-      size_t ja = idx[k];
-      term(bra, interleave(astr[ja], bstr[ib]), wi * W[ja * nb + ib], L, one, two);
-    }
-  }
-  for (int kind = 0; kind < 2; kind++) {
-    const int64_t* off = kind ? tb.d_off : tb.s_off;
-    const int32_t* idx = kind ? tb.d_idx : tb.s_idx;
-    for (int64_t k = off[ib]; k < off[ib + 1]; k++) {
-      size_t jb = idx[k];
-      term(bra, interleave(astr[ia], bstr[jb]), wi * W[ia * nb + jb], L, one, two);
-    }
-  }
-  for (int64_t k = ta.s_off[ia]; k < ta.s_off[ia + 1]; k++) {
-    size_t ja = ta.s_idx[k];
-    for (int64_t m = tb.s_off[ib]; m < tb.s_off[ib + 1]; m++) {
-      size_t jb = tb.s_idx[m];
-      term(bra, interleave(astr[ja], bstr[jb]), wi * W[ja * nb + jb], L, one, two);
-    }
-  }
-}
-
 // Per alpha row: D[ia] = sum_ib W^2 and X[ia][r] = sum_ib W^2 n_r(beta string ib)
 __global__ void row_weights_kernel(const double* __restrict__ W, const uint64_t* __restrict__ bstr, size_t nb,
                                    int L, double* __restrict__ D, double* __restrict__ X) {
@@ -632,9 +492,7 @@ void rdm(sbdgpu_ctx* c, const double* dW, double* one, double* two) {
   double* d_one = (double*)dev_alloc(sizeof(double) * (2 * L2 + 4 * L4));
   double* d_two = d_one + 2 * L2;
   SBD_CUDA(cudaMemsetAsync(d_one, 0, sizeof(double) * (2 * L2 + 4 * L4), c->stream));
-  dim3 g((unsigned)c->na, (unsigned)((c->nb + 127) / 128));
-  rdm_kernel<<<g, 128, 0, c->stream>>>(c->astr, c->bstr, c->na, c->nb, L, dW, c->tab[0], c->tab[1], d_one, d_two);
-  SBD_CUDA(cudaGetLastError());
+  rdm_offdiag(c, dW, d_one, d_two);
   // diagonal contributions (ZeroDiffCorrelation, correlation.h:15-44) from the
   // alpha-row weights, beta-column weights and the alpha x beta occupation moment
   double* Da = (double*)dev_alloc(sizeof(double) * (c->na + c->nb + c->na * L));

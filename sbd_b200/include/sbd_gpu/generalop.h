@@ -557,6 +557,29 @@ void GeneralOp_From_FCIDump(const std::string& filename, MPI_Comm, MPI_Comm, int
 
 namespace gpu {
 
+// Hand both lists of H to a device operator (sbdgpu_genop_set_terms): each
+// field operator as site | dag << 16, in the order written.
+inline int set_terms(sbdgpu_genop* g, const GeneralOp<double>& H) {
+  std::vector<int64_t> doff{0}, ooff{0};
+  std::vector<int32_t> dops, dnd, oops, ond;
+  std::vector<double> dc, oc;
+  auto flat = [](const ProductOp& p, std::vector<int64_t>& off, std::vector<int32_t>& ops, std::vector<int32_t>& nd) {
+    for (size_t k = 0; k < p.size(); k++) ops.push_back(p.op(k).q() | (p.op(k).d() ? 0x10000 : 0));
+    off.push_back((int64_t)ops.size());
+    nd.push_back(p.n_dag());
+  };
+  for (size_t m = 0; m < H.NumNcTerms(); m++) {
+    flat(H.NcTerm((int)m), doff, dops, dnd);
+    dc.push_back(H.NcCoef((int)m));
+  }
+  for (size_t m = 0; m < H.NumOpTerms(); m++) {
+    flat(H.OpTerm((int)m), ooff, oops, ond);
+    oc.push_back(H.OpCoef((int)m));
+  }
+  return sbdgpu_genop_set_terms(g, dc.size(), doff.data(), dops.data(), dnd.data(), dc.data(), oc.size(), ooff.data(),
+                                oops.data(), ond.data(), oc.data());
+}
+
 // The operator and basis on the GPU (sbdgpu_genop): build once, apply many times.
 class DeviceOp {
  public:
@@ -577,26 +600,7 @@ class DeviceOp {
           }
     }
     check(sbdgpu_genop_create(&g_, device, nw_, B.Size(), st.data(), sign ? 1 : 0), "sbdgpu_genop_create");
-    std::vector<int64_t> doff{0}, ooff{0};
-    std::vector<int32_t> dops, dnd, oops, ond;
-    std::vector<double> dc, oc;
-    auto flat = [](const ProductOp& p, std::vector<int64_t>& off, std::vector<int32_t>& ops,
-                   std::vector<int32_t>& nd) {
-      for (size_t k = 0; k < p.size(); k++) ops.push_back(p.op(k).q() | (p.op(k).d() ? 0x10000 : 0));
-      off.push_back((int64_t)ops.size());
-      nd.push_back(p.n_dag());
-    };
-    for (size_t m = 0; m < H.NumNcTerms(); m++) {
-      flat(H.NcTerm((int)m), doff, dops, dnd);
-      dc.push_back(H.NcCoef((int)m));
-    }
-    for (size_t m = 0; m < H.NumOpTerms(); m++) {
-      flat(H.OpTerm((int)m), ooff, oops, ond);
-      oc.push_back(H.OpCoef((int)m));
-    }
-    check(sbdgpu_genop_set_terms(g_, dc.size(), doff.data(), dops.data(), dnd.data(), dc.data(), oc.size(),
-                                 ooff.data(), oops.data(), ond.data(), oc.data()),
-          "sbdgpu_genop_set_terms");
+    check(set_terms(g_, H), "sbdgpu_genop_set_terms");
   }
   ~DeviceOp() { sbdgpu_genop_destroy(g_); }
   DeviceOp(const DeviceOp&) = delete;

@@ -118,6 +118,28 @@ def test_fcidump_operator_equals_tpb_path():
     ctx.close()
 
 
+def test_set_fcidump_equals_oracle_operator():
+    """sbdgpu_genop_set_fcidump (the header's GeneralOp_From_FCIDump, in the
+    library) gives the oracle's operator: the same mult and diagonal."""
+    L, ne = 6, 2
+    ints = synth.make_integrals(L, 13)
+    strs = synth.full_strings(L, ne)
+    states = np.array([int(a) | (int(b) << L) for a in strs for b in strs], dtype=np.uint64)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "FCIDUMP")
+        synth.write_fcidump(p, ints, 2 * ne)
+        norb, _, il = G.read_fcidump(p)
+        g = sbd_b200.GenOp(states, sign=True)
+        assert g.set_fcidump(p) == (L, 2 * ne)
+    H = G.from_fcidump(norb, il)
+    C = np.random.default_rng(3).normal(size=len(states))
+    ref = G.mult(states, H, C)
+    assert np.abs(g.mult(C) - ref).max() <= 1e-12 * np.abs(ref).max()
+    with pytest.raises(sbd_b200.SbdGpuError):
+        g.set_fcidump("/nonexistent/FCIDUMP")
+    g.close()
+
+
 def test_lanczos_matches_oracle():
     L, ne = 4, 2
     _, H = _fcidump_op(L, ne, 9)

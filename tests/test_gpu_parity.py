@@ -89,6 +89,31 @@ def test_rdm(golden):
     assert np.abs(two - golden["rdm2"]).max() < 1e-10
 
 
+@pytest.mark.parametrize("case", ["ragged", "norb40", "wide_beta"])
+def test_rdm_vs_oracle_seeded(case):
+    """1/2-RDMs against the C restatement of Correlation (correlation.h:
+    194-443) on a ragged basis (na != nb), with norb 40 (beta and alpha
+    spectators past orbital 32) and with 15,000 beta strings (rows too wide
+    for the vector row and the strings, or both vector rows, to share shared
+    memory: the kernels read them from L2 instead)."""
+    if case == "ragged":
+        ints, a, b = _seeded_system(14, 4, 300, 11, ragged=True)
+    elif case == "norb40":
+        ints, ne, strs = synth.make_small(40, 3, 150, 17)
+        a = b = np.asarray(strs, np.uint64)
+    else:
+        ints, ne, strs = synth.make_small(20, 5, 15000, 19)
+        b = np.asarray(strs, np.uint64)
+        a = b[:3].copy()
+    ctx = sbd_b200.context_from_integrals(ints, a, b)
+    orc = oracle.Oracle(ints.norb, a, b, ints.ecore, ints.h, ints.eri)
+    W = seeded_vector(ctx.n, 41)
+    one, two = ctx.rdm(W)
+    r1, r2 = orc.correlation(W)
+    assert np.abs(one - r1).max() < 1e-11
+    assert np.abs(two - r2).max() < 1e-11
+
+
 def _seeded_system(norb, ne, count, seed, ragged=False):
     ints, ne, strs = synth.make_small(norb, ne, count, seed)
     a = strs
