@@ -321,7 +321,7 @@ int sbdgpu_genop_set_fcidump(sbdgpu_genop* g, const char* path, int* norb, int* 
 
 /* W += H C (mult.h:268-291 at one rank: the diagonal list, then the
  * off-diagonal one).  Host vectors of nstates doubles; the _device form takes
- * device pointers and runs on the object's stream. */
+ * device pointers, runs on the object's stream and returns when it is done. */
 int sbdgpu_genop_mult(sbdgpu_genop* g, const double* C, double* W);
 int sbdgpu_genop_mult_device(sbdgpu_genop* g, const double* dC, double* dW);
 

@@ -612,6 +612,7 @@ int sbdgpu_genop_mult_device(sbdgpu_genop* g, const double* dC, double* dW) {
   return guarded(g, [&] {
     if (!dC || !dW) throw Error{SBDGPU_ERR_ARG, "null vector"};
     mult(g, dC, dW);
+    SBD_CUDA(cudaStreamSynchronize(g->base.stream));
   });
 }
 

@@ -79,7 +79,10 @@ void davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, double* Wh,
     return true;
   };
 
-  // initial basis: the caller's vectors, or the nroots lowest-H_ii determinants
+  // initial basis: the caller's vectors, or determinant 0 (the reference's
+  // start vector, davidson.h:120-135) and the lowest-H_ii determinants.  The
+  // lowest-H_ii determinants alone can miss the ground state's symmetry
+  // sector altogether (at 144M determinants they found a root 26 Eh above it).
   int m = 0;
   {
     double w2 = 0.0;
@@ -99,6 +102,7 @@ void davidson_roots(sbdgpu_ctx* c, const sbdgpu_opts* o, int nroots, double* Wh,
       std::iota(order.begin(), order.end(), (size_t)0);
       std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return h[a] < h[b]; });
       const double one = 1.0;
+      std::stable_partition(order.begin(), order.end(), [](size_t a) { return a == 0; });
       for (size_t q = 0; q < n && m < nroots; q++) {
         SBD_CUDA(cudaMemsetAsync(C[m], 0, sizeof(double) * n, st));
         SBD_CUDA(cudaMemcpyAsync(C[m] + order[q], &one, sizeof(double), cudaMemcpyHostToDevice, st));
