@@ -163,7 +163,7 @@ int sbdgpu_sigma_device_noalloc(sbdgpu_ctx* ctx, const double* dC, double* dsigm
  * every residual norm is below opts->eps, after opts->max_it cycles, or at
  * opts->max_time seconds.
  *   W         [nroots][na*nb], reference convention.  In: initial vectors, or
- *             all zeros for the nroots lowest-H_ii determinants.  Out: the
+ *             all zeros for determinant 0 and the lowest-H_ii determinants.  Out: the
  *             normalised Ritz vectors.
  *   energies  out [nroots]: Ritz values, ascending
  *   resid     out [nroots] (may be NULL): residual norms
@@ -172,13 +172,18 @@ int sbdgpu_davidson_roots(sbdgpu_ctx* ctx, const sbdgpu_opts* opts, int nroots, 
                           double* resid, int* n_iter, int* n_sigma);
 
 /* Lowest-root Davidson (as sbdgpu_davidson, same opts) for nprob independent
- * problems at once: a pool of max_threads host threads (0: one per problem,
- * capped at the host's hardware threads and at 32)
- * drives the contexts, each on its own stream, so their kernels overlap on the
- * GPU.  W[i]: problem i's initial vector in, Ritz vector out (reference
- * convention); energies[i], n_steps[i] (may be NULL) and status[i] (may be
- * NULL) per problem.  Returns SBDGPU_OK, or the first problem's error status.
- * The contexts must be distinct and not used by other threads meanwhile. */
+ * problems at once (an extension; the reference has none).  FP64 contexts on
+ * one device run a device-resident Davidson: every step of a problem (its
+ * correction, Gram-Schmidt, sigma, projected row, small eigenproblem, Ritz
+ * update and norms) is one replayed CUDA graph on the context's stream, one
+ * host thread launches a step for every unconverged problem and waits once
+ * per round, and all vectors come from one device allocation made before the
+ * first round.  Other precisions, stored Hamiltonians or several devices run
+ * each problem's sbdgpu_davidson in turn.  W[i]: problem i's initial vector
+ * in, Ritz vector out (reference convention); energies[i], n_steps[i] (may be
+ * NULL) and status[i] (may be NULL) per problem.  Returns SBDGPU_OK or the
+ * first error status.  The contexts must be distinct and not used by other
+ * threads meanwhile.  max_threads is not used (kept for the signature). */
 int sbdgpu_davidson_batch(int nprob, sbdgpu_ctx* const* ctxs, const sbdgpu_opts* opts, double* const* W,
                           double* energies, int* n_steps, int* status, int max_threads);
 
@@ -272,6 +277,19 @@ int sbdgpu_precond_apply(sbdgpu_ctx* ctx, const double* R, double e0, double* ou
 int sbdgpu_mlp_loss_grad(int device, const float* w, int B, const float* X, const double* r, const double* den,
                          const double* u, const double* t, const double* wt, double S, double eps_reg,
                          double* loss, float* grad);
+
+/* Launch shape of the FP64 alpha-beta kernel (an extension): ab_group alpha
+ * singles per CTA (16, 8, 4, 2 or 1, where the integral block fits in shared
+ * memory beside a row of C) and ab_threads threads per CTA (128, 256, 512 or
+ * 1024); (0, 0) restores the default (the largest group that fits; 512
+ * threads while two CTAs fit an SM, else 1024).  A shape that does not fit the
+ * basis is refused. */
+int sbdgpu_set_tuning(sbdgpu_ctx* ctx, int ab_group, int ab_threads);
+
+/* Time every alpha-beta shape that fits (reps FP64 sigma builds each, after
+ * one warm-up) and keep the fastest on the context; its shape and sigma time
+ * in *ab_group, *ab_threads, *best_ms (each may be NULL). */
+int sbdgpu_autotune(sbdgpu_ctx* ctx, int reps, int* ab_group, int* ab_threads, float* best_ms);
 
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);
 void sbdgpu_destroy(sbdgpu_ctx* ctx);

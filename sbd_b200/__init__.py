@@ -31,7 +31,8 @@ EXPORTS = [
     "sbdgpu_precond_train", "sbdgpu_precond_get", "sbdgpu_precond_set", "sbdgpu_precond_apply",
     "sbdgpu_mlp_loss_grad", "sbdgpu_genop_create", "sbdgpu_genop_set_terms", "sbdgpu_genop_mult",
     "sbdgpu_genop_mult_device", "sbdgpu_genop_diagonal", "sbdgpu_genop_lanczos", "sbdgpu_genop_davidson",
-    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy", "sbdgpu_genop_set_fcidump",
+    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy", "sbdgpu_genop_set_fcidump", "sbdgpu_set_tuning",
+    "sbdgpu_autotune",
 ]
 
 PRECOND_DIAGONAL = 0
@@ -90,6 +91,9 @@ def lib():
         L.sbdgpu_precond_apply.argtypes = [_vp, _dp, ctypes.c_double, _dp]
         L.sbdgpu_mlp_loss_grad.argtypes = [ctypes.c_int, _fp, ctypes.c_int, _fp, _dp, _dp, _dp, _dp, _dp,
                                            ctypes.c_double, ctypes.c_double, _dp, _fp]
+        L.sbdgpu_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+        L.sbdgpu_autotune.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_float)]
         L.sbdgpu_store_hamiltonian.argtypes = [_vp, _u64p]
         L.sbdgpu_release_hamiltonian.argtypes = [_vp]
         L.sbdgpu_rdm.argtypes = [_vp, _dp, _dp, _dp]
@@ -216,6 +220,17 @@ class Context:
         st = (ctypes.c_int * 2)()
         self._check(lib().sbdgpu_wait_selftest(self._h, int(spin_limit), st))
         return int(st[0]), int(st[1])
+
+    def set_tuning(self, ab_group: int, ab_threads: int) -> None:
+        """Launch shape of the FP64 alpha-beta kernel ((0, 0): the default)."""
+        self._check(lib().sbdgpu_set_tuning(self._h, int(ab_group), int(ab_threads)))
+
+    def autotune(self, reps: int = 3):
+        """Time every alpha-beta shape that fits, keep the fastest:
+        (ab_group, ab_threads, sigma ms)."""
+        g, t, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0.0)
+        self._check(lib().sbdgpu_autotune(self._h, int(reps), ctypes.byref(g), ctypes.byref(t), ctypes.byref(ms)))
+        return g.value, t.value, ms.value
 
     def store_hamiltonian(self) -> int:
         """Method 1: keep the Hamiltonian's off-diagonal elements on the device

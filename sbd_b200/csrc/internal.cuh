@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "sbdgpu.h"
@@ -104,6 +105,8 @@ struct sbdgpu_ctx {
   int blk_max = 0;
   size_t blk_r0 = 0, blk_r1 = 0;
   sbdgpu::SpinTables tab[2];
+  // alpha-beta launch shape of the FP64 sigma (0: the shared-memory heuristic)
+  int ab_group = 0, ab_threads = 0;
   // RDM tables: beta singles grouped by excitation, bra row of every alpha single
   int64_t* rdm_bin_off = nullptr;
   uint32_t* rdm_bin_ent = nullptr;
@@ -147,6 +150,7 @@ template <typename T>
 void transpose_add(const T* in, T* out, size_t rows, size_t cols, cudaStream_t s);
 void ensure_fp32(sbdgpu_ctx* c);
 double dot(sbdgpu_ctx* c, const double* x, const double* y, size_t n);
+void dot_device(sbdgpu_ctx* c, const double* x, const double* y, size_t n, double* out);  // needs ensure_scratch
 void scale(double* x, double a, size_t n, cudaStream_t s);
 double dot_f(sbdgpu_ctx* c, const float* x, const double* xd, const float* y, size_t n);
 void axpy_df(double* y, const float* x, double a, size_t n, cudaStream_t s);
@@ -165,6 +169,8 @@ void rdm(sbdgpu_ctx* c, const double* dW, double* one, double* two);
 void rdm_offdiag(sbdgpu_ctx* c, const double* dW, double* one, double* two);
 void ensure_rdm_tables(sbdgpu_ctx* c);
 void free_rdm_tables(sbdgpu_ctx* c);
+// sigma.cu: the alpha-beta launch shapes (group size, threads) open to this context's FP64 sigma
+std::vector<std::pair<int, int>> ab_shapes(sbdgpu_ctx* c);
 // genop.cu: record an error message on a generic-path object
 void genop_set_error(sbdgpu_genop* g, const std::string& msg);
 void occupation(sbdgpu_ctx* c, const double* dW, double* dens);

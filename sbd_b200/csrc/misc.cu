@@ -381,6 +381,13 @@ double dot(sbdgpu_ctx* c, const double* x, const double* y, size_t n) {
   return r;
 }
 
+// <x|y> into device memory *out, on the context's stream, without waiting
+void dot_device(sbdgpu_ctx* c, const double* x, const double* y, size_t n, double* out) {
+  dot_partial<<<kRedBlocks, kRedThreads, 0, c->stream>>>(x, y, n, c->red);
+  dot_final<<<1, 1024, 0, c->stream>>>(c->red, kRedBlocks, out);
+  SBD_CUDA(cudaGetLastError());
+}
+
 double dot_f(sbdgpu_ctx* c, const float* x, const double* xd, const float* y, size_t n) {
   ensure_scratch(c);
   dot_partial_f<<<kRedBlocks, kRedThreads, 0, c->stream>>>(x, y, xd, n, c->red);

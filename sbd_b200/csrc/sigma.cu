@@ -311,25 +311,56 @@ struct AlphaSingles {
   size_t ia0;
 };
 
-template <typename T, int G>
-void launch_ab(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem, const AlphaSingles& as) {
+template <typename T, int G, int NT>
+void launch_ab_nt(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem, const AlphaSingles& as) {
   const SpinTables& tb = c->tab[1];
   dim3 grid((unsigned)c->na, (unsigned)((as.max_s + G - 1) / G));
   if (grid.y == 0) return;
-  if (2 * (smem + 1024) <= 228 * 1024) {
-    allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<T, G, 512>), c->device);
-    ab_kernel<T, G, 512><<<grid, 512, smem, c->stream>>>(C, S, c->nb, c->P, vf, as.off, as.idx, as.info,
-                                                         tb.sell_off, tb.sell_w, tb.sell, tb.nslice, as.ia0);
-  } else {
-    allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<T, G, 1024>), c->device);
-    ab_kernel<T, G, 1024><<<grid, 1024, smem, c->stream>>>(C, S, c->nb, c->P, vf, as.off, as.idx, as.info,
-                                                           tb.sell_off, tb.sell_w, tb.sell, tb.nslice, as.ia0);
-  }
+  allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<T, G, NT>), c->device);
+  ab_kernel<T, G, NT><<<grid, NT, smem, c->stream>>>(C, S, c->nb, c->P, vf, as.off, as.idx, as.info, tb.sell_off,
+                                                     tb.sell_w, tb.sell, tb.nslice, as.ia0);
   SBD_CUDA(cudaGetLastError());
 }
 
-// The alpha-beta term: the largest group of alpha singles per CTA whose
-// integral block fits in shared memory next to one row of C.
+// threads per CTA: the tuned choice, else 512 while two CTAs fit an SM's
+// shared memory and 1024 when only one does
+template <typename T, int G>
+void launch_ab(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem, const AlphaSingles& as, int nt) {
+  if (nt == 0) nt = 2 * (smem + 1024) <= 228 * 1024 ? 512 : 1024;
+  switch (nt) {
+    case 128: launch_ab_nt<T, G, 128>(c, C, S, vf, smem, as); break;
+    case 256: launch_ab_nt<T, G, 256>(c, C, S, vf, smem, as); break;
+    case 512: launch_ab_nt<T, G, 512>(c, C, S, vf, smem, as); break;
+    default: launch_ab_nt<T, G, 1024>(c, C, S, vf, smem, as); break;
+  }
+}
+
+}  // namespace
+
+// Alpha-beta launch shapes an FP64 sigma of this context can take: group
+// sizes whose integral block fits in shared memory next to one row of C,
+// times 128 / 256 / 512 / 1024 threads per CTA.
+std::vector<std::pair<int, int>> ab_shapes(sbdgpu_ctx* c) {
+  int dev_smem = 0;
+  SBD_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  const size_t budget = (size_t)dev_smem - 1024;
+  std::vector<std::pair<int, int>> out;
+  const int groups[5] = {16, 8, 4, 2, 1};
+  const size_t sm[5] = {ab_smem<double, 16>(c->nb, c->P), ab_smem<double, 8>(c->nb, c->P),
+                        ab_smem<double, 4>(c->nb, c->P), ab_smem<double, 2>(c->nb, c->P),
+                        ab_smem<double, 1>(c->nb, c->P)};
+  for (int k = 0; k < 5; k++)
+    if (sm[k] <= budget)
+      for (int nt : {128, 256, 512, 1024}) out.emplace_back(groups[k], nt);
+  return out;
+}
+
+namespace {
+
+// The alpha-beta term: the context's tuned group size and threads for FP64
+// when set (sbdgpu_set_tuning / sbdgpu_autotune), else the largest group of
+// alpha singles per CTA whose integral block fits in shared memory next to
+// one row of C.
 template <typename T>
 void alpha_beta(sbdgpu_ctx* c, const T* C, T* S, const T* vf, const AlphaSingles& as) {
   int dev_smem = 0;
@@ -338,16 +369,18 @@ void alpha_beta(sbdgpu_ctx* c, const T* C, T* S, const T* vf, const AlphaSingles
   if (c->nb > 65536) throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: more than 65536 beta strings"};
   size_t nb = c->nb;
   int P = c->P;
-  if (ab_smem<T, 16>(nb, P) <= budget)
-    launch_ab<T, 16>(c, C, S, vf, ab_smem<T, 16>(nb, P), as);
-  else if (ab_smem<T, 8>(nb, P) <= budget)
-    launch_ab<T, 8>(c, C, S, vf, ab_smem<T, 8>(nb, P), as);
-  else if (ab_smem<T, 4>(nb, P) <= budget)
-    launch_ab<T, 4>(c, C, S, vf, ab_smem<T, 4>(nb, P), as);
-  else if (ab_smem<T, 2>(nb, P) <= budget)
-    launch_ab<T, 2>(c, C, S, vf, ab_smem<T, 2>(nb, P), as);
-  else if (ab_smem<T, 1>(nb, P) <= budget)
-    launch_ab<T, 1>(c, C, S, vf, ab_smem<T, 1>(nb, P), as);
+  const bool tuned = sizeof(T) == 8 && c->ab_group > 0;
+  const int g = tuned ? c->ab_group : 0, nt = tuned ? c->ab_threads : 0;
+  if ((g == 0 || g == 16) && ab_smem<T, 16>(nb, P) <= budget)
+    launch_ab<T, 16>(c, C, S, vf, ab_smem<T, 16>(nb, P), as, nt);
+  else if ((g == 0 || g == 8) && ab_smem<T, 8>(nb, P) <= budget)
+    launch_ab<T, 8>(c, C, S, vf, ab_smem<T, 8>(nb, P), as, nt);
+  else if ((g == 0 || g == 4) && ab_smem<T, 4>(nb, P) <= budget)
+    launch_ab<T, 4>(c, C, S, vf, ab_smem<T, 4>(nb, P), as, nt);
+  else if ((g == 0 || g == 2) && ab_smem<T, 2>(nb, P) <= budget)
+    launch_ab<T, 2>(c, C, S, vf, ab_smem<T, 2>(nb, P), as, nt);
+  else if ((g == 0 || g == 1) && ab_smem<T, 1>(nb, P) <= budget)
+    launch_ab<T, 1>(c, C, S, vf, ab_smem<T, 1>(nb, P), as, nt);
   else
     throw Error{SBDGPU_ERR_LIMIT, "alpha-beta kernel: one beta row and integral row exceed shared memory"};
 }
@@ -373,6 +406,8 @@ void sigma_launch(sbdgpu_ctx* c, const T* C, T* S, T* ct, T* st, const T* ja, co
 
 template <int G>
 void preload_ab(int device) {
+  allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<double, G, 128>), device);
+  allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<double, G, 256>), device);
   allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<double, G, 512>), device);
   allow_dynamic_smem(reinterpret_cast<const void*>(ab_kernel<double, G, 1024>), device);
 }

@@ -1,7 +1,9 @@
-"""Many independent problems in one sbdgpu_davidson_batch call: the same
-energies and ground states as running each problem alone (and the
-reference's energy on its own fixture), with one thread per problem or a
-bounded pool."""
+"""Many independent problems in one sbdgpu_davidson_batch call (the
+device-resident Davidson with replayed step graphs): the same energies, ground
+states and step counts as running each problem alone (and the reference's
+energy on its own fixture); the mixed-precision form runs each problem in
+turn.  The alpha-beta launch shapes (sbdgpu_set_tuning, sbdgpu_autotune) give
+the default sigma."""
 import numpy as np
 import pytest
 
@@ -48,3 +50,42 @@ def test_batch_rejects_a_context_given_twice():
     c = gpu_ctx(g)
     with pytest.raises(sbd_b200.SbdGpuError, match="twice"):
         sbd_b200.davidson_batch([c, c], [_unit(c.n), _unit(c.n)], 10, 10, 1e-6)
+
+
+def test_batch_step_counts_follow_single_runs():
+    ctxs, g = _contexts()
+    W0 = [_unit(c.n) for c in ctxs]
+    E, Ws, steps = sbd_b200.davidson_batch(ctxs, W0, 300, 8, 1e-9)
+    for c, e, s in zip(ctxs, E, steps):
+        e1, _, te, _ = c.davidson(_unit(c.n), 300, 8, 1e-9)
+        assert abs(e - e1) < 1e-10
+        assert abs(s - len(te)) <= 2, (s, len(te))
+
+
+def test_batch_mixed_precision_runs_each_problem():
+    ctxs, g = _contexts()
+    E, Ws, steps = sbd_b200.davidson_batch(ctxs[:3], [_unit(c.n) for c in ctxs[:3]], 300, 10, 1e-6,
+                                           precision=sbd_b200.MIXED)
+    for c, e in zip(ctxs[:3], E):
+        e1, _, _, _ = c.davidson(_unit(c.n), 300, 10, 1e-9)
+        assert abs(e - e1) < 1e-8
+
+
+def test_alpha_beta_shapes_give_the_default_sigma():
+    ints, a, b = _seeded_system(14, 4, 300, 11, False)
+    c = sbd_b200.context_from_integrals(ints, a, b)
+    C = np.random.default_rng(7).normal(size=c.n)
+    ref = c.sigma(C)
+    for g, t in [(1, 128), (2, 256), (4, 512), (8, 1024), (16, 128)]:
+        c.set_tuning(g, t)
+        got = c.sigma(C)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (g, t)
+    with pytest.raises(sbd_b200.SbdGpuError):
+        c.set_tuning(3, 256)
+    with pytest.raises(sbd_b200.SbdGpuError):
+        c.set_tuning(4, 200)
+    g, t, ms = c.autotune(2)
+    assert g in (1, 2, 4, 8, 16) and t in (128, 256, 512, 1024) and ms > 0
+    np.testing.assert_allclose(c.sigma(C), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    c.set_tuning(0, 0)
+    c.close()
