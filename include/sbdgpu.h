@@ -362,6 +362,22 @@ int sbdgpu_genop_lanczos(sbdgpu_genop* g, double* W, int max_it, double eps, dou
 int sbdgpu_genop_davidson(sbdgpu_genop* g, const sbdgpu_opts* opts, double* W, double* energy, double* trace_e,
                           double* trace_tol, int max_trace, int* n_steps);
 
+/* <W|H^2|W> as MeasHamSquare computes it (expand.h:10-215): every basis
+ * state weighted by the diagonal list, every configuration an off-diagonal
+ * term reaches from basis state i weighted coef * sign * W_i (inside the basis
+ * or not), equal configurations summed, then the sum of squares.  W: host
+ * vector of nstates doubles. */
+int sbdgpu_genop_ham_square(sbdgpu_genop* g, const double* W, double* res);
+
+/* The expanded basis of ExpandBasis (expand.h:217-366): the basis states and
+ * every configuration an off-diagonal term reaches from basis state i with
+ * |coef * sign * W_i| > eps_hb, distinct, ascending as nwords-word integers
+ * (word nwords-1 most significant).  *n_out receives their number; with out
+ * == NULL nothing else is written, else out must hold capacity >= *n_out
+ * states of nwords words (SBDGPU_ERR_LIMIT otherwise). */
+int sbdgpu_genop_expand(sbdgpu_genop* g, const double* W, double eps_hb, uint64_t* out, size_t capacity,
+                        size_t* n_out);
+
 const char* sbdgpu_genop_last_error(sbdgpu_genop* g);
 void sbdgpu_genop_destroy(sbdgpu_genop* g);
 

@@ -302,3 +302,58 @@ def read_fcidump(path):
     norb = int(tok[tok.index("NORB") + 2]) if "NORB" in tok else None
     nelec = int(tok[tok.index("NELEC") + 2]) if "NELEC" in tok else None
     return norb, nelec, ints
+
+
+def _targets(v, ops, sign):
+    """The state reached from bra v by one off-diagonal term (mult.h:213-240)
+    and its sign, or None."""
+    nd = sum(1 for d, _ in ops if d)
+    w, s = v, 1
+    for k, (_, q) in enumerate(ops):
+        if k < nd:
+            if not (w >> q) & 1:
+                return None
+            w &= ~(1 << q)
+        else:
+            if (w >> q) & 1:
+                return None
+            w |= 1 << q
+        if sign and bin(w & ((1 << q) - 1)).count("1") & 1:
+            s = -s
+    return w, s
+
+
+def ham_square(states, H, W, sign=True):
+    """MeasHamSquare (expand.h:10-215): every basis state weighted by the
+    diagonal list, every off-diagonal target weighted coef * sign * W_i, equal
+    configurations summed, then the sum of squares."""
+    st = np.asarray(states, dtype=np.uint64)
+    ints = [_state_int(st, i) for i in range(st.shape[0])]
+    diag, off = H
+    acc = {}
+    for i, v in enumerate(ints):
+        val = 0.0
+        for c, ops in diag:
+            nd = sum(1 for d, _ in ops if d)
+            if all((v >> q) & 1 for _, q in ops[:nd]):
+                val += c * W[i]
+        acc[v] = acc.get(v, 0.0) + val
+        for c, ops in off:
+            t = _targets(v, ops, sign)
+            if t is not None:
+                acc[t[0]] = acc.get(t[0], 0.0) + c * t[1] * W[i]
+    return float(sum(x * x for x in acc.values()))
+
+
+def expand(states, H, W, eps_hb, sign=True):
+    """ExpandBasis (expand.h:217-366): the basis plus every off-diagonal
+    target with |coef * sign * W_i| > eps_hb, sorted ascending as integers."""
+    st = np.asarray(states, dtype=np.uint64)
+    ints = [_state_int(st, i) for i in range(st.shape[0])]
+    out = set(ints)
+    for i, v in enumerate(ints):
+        for c, ops in H[1]:
+            t = _targets(v, ops, sign)
+            if t is not None and abs(c * t[1] * W[i]) > eps_hb:
+                out.add(t[0])
+    return sorted(out)

@@ -31,7 +31,7 @@ EXPORTS = [
     "sbdgpu_precond_train", "sbdgpu_precond_get", "sbdgpu_precond_set", "sbdgpu_precond_apply",
     "sbdgpu_mlp_loss_grad", "sbdgpu_genop_create", "sbdgpu_genop_set_terms", "sbdgpu_genop_mult",
     "sbdgpu_genop_mult_device", "sbdgpu_genop_diagonal", "sbdgpu_genop_lanczos", "sbdgpu_genop_davidson",
-    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy", "sbdgpu_genop_set_fcidump", "sbdgpu_set_tuning",
+    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy", "sbdgpu_genop_set_fcidump", "sbdgpu_set_tuning", "sbdgpu_genop_ham_square", "sbdgpu_genop_expand",
     "sbdgpu_autotune",
 ]
 
@@ -111,6 +111,9 @@ def lib():
         L.sbdgpu_genop_set_fcidump.argtypes = [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
                                                ctypes.POINTER(ctypes.c_int)]
         L.sbdgpu_genop_mult.argtypes = [_vp, _dp, _dp]
+        L.sbdgpu_genop_ham_square.argtypes = [_vp, _dp, _dp]
+        L.sbdgpu_genop_expand.argtypes = [_vp, _dp, ctypes.c_double, _u64p, ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_size_t)]
         L.sbdgpu_genop_mult_device.argtypes = [_vp, _vp, _vp]
         L.sbdgpu_genop_diagonal.argtypes = [_vp, _dp]
         L.sbdgpu_genop_lanczos.argtypes = [_vp, _dp, ctypes.c_int, ctypes.c_double, _dp,
@@ -436,6 +439,23 @@ class GenOp:
 
     def mult_device(self, dC_ptr: int, dW_ptr: int) -> None:
         self._check(lib().sbdgpu_genop_mult_device(self._h, _vp(dC_ptr), _vp(dW_ptr)))
+
+    def ham_square(self, W: np.ndarray) -> float:
+        """<W|H^2|W> over the expanded space (MeasHamSquare)."""
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        r = ctypes.c_double(0.0)
+        self._check(lib().sbdgpu_genop_ham_square(self._h, _p(W, _dp), ctypes.byref(r)))
+        return r.value
+
+    def expand(self, W: np.ndarray, eps_hb: float) -> np.ndarray:
+        """The expanded basis (ExpandBasis): uint64 [m, nwords], ascending."""
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        m = ctypes.c_size_t(0)
+        self._check(lib().sbdgpu_genop_expand(self._h, _p(W, _dp), float(eps_hb), None, 0, ctypes.byref(m)))
+        out = np.zeros((m.value, self.nwords), dtype=np.uint64)
+        self._check(lib().sbdgpu_genop_expand(self._h, _p(W, _dp), float(eps_hb), _p(out, _u64p), m.value,
+                                              ctypes.byref(m)))
+        return out
 
     def diagonal(self) -> np.ndarray:
         out = np.empty(self.n)

@@ -31,6 +31,9 @@
 #include <iostream>
 #include <numeric>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include "internal.cuh"
 
 using sbdgpu::Error;
@@ -530,6 +533,199 @@ void davidson(sbdgpu_genop* g, const sbdgpu_opts* o, double* Wh, double* energy,
   if (n_steps) *n_steps = steps;
 }
 
+
+// ---------------------------------------------------------------- the expanded space
+//
+// MeasHamSquare and ExpandBasis (expand.h:10-366) look past the basis: every
+// configuration an off-diagonal term reaches from a basis state, with weight
+// coef * sign * W_i.  Here a count pass and a write pass lay those out (with
+// the basis states themselves first), a least-significant-word-first radix
+// sort of their indices (CUB) orders them by configuration, and head flags
+// mark each distinct configuration.
+
+constexpr int kGenThreads = 256;
+
+// entries of state i: 1 (itself) + its applicable off-diagonal terms (with
+// |coef sign W_i| > eps when select)
+template <int NW>
+__global__ void __launch_bounds__(kGenThreads) gen_count_kernel(const uint64_t* __restrict__ states, size_t n,
+                                                               const Term<NW>* __restrict__ terms, size_t n_terms,
+                                                               int sign, const double* __restrict__ W, double eps,
+                                                               int select, int64_t* __restrict__ counts) {
+  const size_t i = (size_t)blockIdx.x * kGenThreads + threadIdx.x;
+  if (i >= n) return;
+  uint64_t v[NW];
+#pragma unroll
+  for (int x = 0; x < NW; x++) v[x] = states[i * NW + x];
+  const double wi = W[i];
+  int64_t cnt = 1;
+  for (size_t k = 0; k < n_terms; k++) {
+    uint64_t w[NW];
+    double s;
+    if (!apply_term<NW>(terms[k], v, sign, w, &s)) continue;
+    if (!select || fabs(terms[k].coef * s * wi) > eps) cnt++;
+  }
+  counts[i] = cnt;
+}
+
+template <int NW>
+__global__ void __launch_bounds__(kGenThreads) gen_write_kernel(const uint64_t* __restrict__ states, size_t n,
+                                                               const Term<NW>* __restrict__ terms, size_t n_terms,
+                                                               int sign, const double* __restrict__ W,
+                                                               const double* __restrict__ hdiag, double eps, int select,
+                                                               const int64_t* __restrict__ offs,
+                                                               uint64_t* __restrict__ keys, double* __restrict__ vals) {
+  const size_t i = (size_t)blockIdx.x * kGenThreads + threadIdx.x;
+  if (i >= n) return;
+  uint64_t v[NW];
+#pragma unroll
+  for (int x = 0; x < NW; x++) v[x] = states[i * NW + x];
+  const double wi = W[i];
+  int64_t o = offs[i];
+#pragma unroll
+  for (int x = 0; x < NW; x++) keys[(size_t)o * NW + x] = v[x];
+  vals[o++] = hdiag[i] * wi;  // the diagonal list's weight (expand.h:43-64)
+  for (size_t k = 0; k < n_terms; k++) {
+    uint64_t w[NW];
+    double s;
+    if (!apply_term<NW>(terms[k], v, sign, w, &s)) continue;
+    const double val = terms[k].coef * s * wi;
+    if (select && !(fabs(val) > eps)) continue;
+#pragma unroll
+    for (int x = 0; x < NW; x++) keys[(size_t)o * NW + x] = w[x];
+    vals[o++] = val;
+  }
+}
+
+__global__ void gather_word_kernel(const uint64_t* __restrict__ keys, int nw, int word,
+                                   const int64_t* __restrict__ idx, uint64_t* __restrict__ out, size_t m) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = keys[(size_t)idx[i] * nw + word];
+}
+
+// head[i] = 1 where sorted entry i starts a new configuration
+__global__ void head_kernel(const uint64_t* __restrict__ keys, int nw, const int64_t* __restrict__ idx,
+                            int64_t* __restrict__ head, size_t m) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+    int64_t h = i == 0;
+    if (i > 0)
+      for (int x = 0; x < nw; x++) h |= keys[(size_t)idx[i] * nw + x] != keys[(size_t)idx[i - 1] * nw + x];
+    head[i] = h;
+  }
+}
+
+// sums[seg[i]] += vals[idx[i]] (seg = inclusive scan of head - 1)
+__global__ void seg_sum_kernel(const int64_t* __restrict__ seg, const int64_t* __restrict__ idx,
+                               const double* __restrict__ vals, double* __restrict__ sums, size_t m) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+    atomicAdd(&sums[seg[i] - 1], vals[idx[i]]);
+}
+
+// out[seg[i]-1] = key of entry i for the heads
+__global__ void compact_kernel(const uint64_t* __restrict__ keys, int nw, const int64_t* __restrict__ idx,
+                               const int64_t* __restrict__ head, const int64_t* __restrict__ seg,
+                               uint64_t* __restrict__ out, size_t m) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+    if (head[i])
+      for (int x = 0; x < nw; x++) out[(size_t)(seg[i] - 1) * nw + x] = keys[(size_t)idx[i] * nw + x];
+}
+
+}  // namespace
+
+
+namespace {
+
+// The expanded space of W: sorted entry indices (idx), their configuration
+// keys, weights, head flags and segment numbers (inclusive scan of the
+// heads), all on the device; returns the number of distinct configurations.
+struct Expanded {
+  std::vector<void*> bufs;
+  cudaStream_t s = nullptr;
+  uint64_t* keys = nullptr;
+  double* vals = nullptr;
+  int64_t* idx = nullptr;
+  int64_t* head = nullptr;
+  int64_t* seg = nullptr;
+  size_t m = 0, distinct = 0;
+  void* alloc(size_t bytes) {
+    bufs.push_back(sbdgpu::dev_alloc(std::max<size_t>(bytes, 16)));
+    return bufs.back();
+  }
+  ~Expanded() {
+    if (s) cudaStreamSynchronize(s);
+    for (auto p : bufs) cudaFree(p);
+  }
+};
+
+template <int NW>
+void expand_nw(sbdgpu_genop* g, const double* dW, double eps, int select, Expanded& x) {
+  cudaStream_t st = g->base.stream;
+  x.s = st;
+  const size_t n = g->n;
+  const unsigned nblk = (unsigned)((n + kGenThreads - 1) / kGenThreads);
+  const Term<NW>* terms = static_cast<const Term<NW>*>(g->terms);
+  int64_t* counts = (int64_t*)x.alloc(sizeof(int64_t) * (n + 1));
+  int64_t* offs = (int64_t*)x.alloc(sizeof(int64_t) * (n + 1));
+  SBD_CUDA(cudaMemsetAsync(counts + n, 0, sizeof(int64_t), st));
+  gen_count_kernel<NW><<<nblk, kGenThreads, 0, st>>>(g->states, n, terms, g->n_terms, g->sign, dW, eps, select,
+                                                     counts);
+  SBD_CUDA(cudaGetLastError());
+  size_t tb = 0;
+  SBD_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, counts, offs, n + 1, st));
+  void* tmp = x.alloc(tb);
+  SBD_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, counts, offs, n + 1, st));
+  int64_t m = 0;
+  SBD_CUDA(cudaMemcpyAsync(&m, offs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  SBD_CUDA(cudaStreamSynchronize(st));
+  x.m = (size_t)m;
+  x.keys = (uint64_t*)x.alloc(sizeof(uint64_t) * x.m * NW);
+  x.vals = (double*)x.alloc(sizeof(double) * x.m);
+  gen_write_kernel<NW><<<nblk, kGenThreads, 0, st>>>(g->states, n, terms, g->n_terms, g->sign, dW, g->hdiag, eps,
+                                                     select, offs, x.keys, x.vals);
+  SBD_CUDA(cudaGetLastError());
+  // sort the entry indices by configuration, least significant word first
+  // (each radix pass is stable)
+  int64_t* ia = (int64_t*)x.alloc(sizeof(int64_t) * x.m);
+  int64_t* ib = (int64_t*)x.alloc(sizeof(int64_t) * x.m);
+  uint64_t* ka = (uint64_t*)x.alloc(sizeof(uint64_t) * x.m);
+  uint64_t* kb = (uint64_t*)x.alloc(sizeof(uint64_t) * x.m);
+  std::vector<int64_t> iota(x.m);
+  for (size_t i = 0; i < x.m; i++) iota[i] = (int64_t)i;
+  SBD_CUDA(cudaMemcpyAsync(ia, iota.data(), sizeof(int64_t) * x.m, cudaMemcpyHostToDevice, st));
+  const unsigned gb = (unsigned)std::min<size_t>((x.m + 255) / 256 + 1, 148 * 8);
+  size_t tsort = 0;
+  SBD_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tsort, ka, kb, ia, ib, x.m, 0, 64, st));
+  void* tmp2 = x.alloc(tsort);
+  for (int w = 0; w < NW; w++) {
+    gather_word_kernel<<<gb, 256, 0, st>>>(x.keys, NW, w, ia, ka, x.m);
+    SBD_CUDA(cudaGetLastError());
+    SBD_CUDA(cub::DeviceRadixSort::SortPairs(tmp2, tsort, ka, kb, ia, ib, x.m, 0, 64, st));
+    std::swap(ia, ib);
+  }
+  x.idx = ia;
+  x.head = (int64_t*)x.alloc(sizeof(int64_t) * x.m);
+  x.seg = (int64_t*)x.alloc(sizeof(int64_t) * x.m);
+  head_kernel<<<gb, 256, 0, st>>>(x.keys, NW, x.idx, x.head, x.m);
+  SBD_CUDA(cudaGetLastError());
+  size_t ts = 0;
+  SBD_CUDA(cub::DeviceScan::InclusiveSum(nullptr, ts, x.head, x.seg, x.m, st));
+  void* tmp3 = x.alloc(ts);
+  SBD_CUDA(cub::DeviceScan::InclusiveSum(tmp3, ts, x.head, x.seg, x.m, st));
+  int64_t d = 0;
+  SBD_CUDA(cudaMemcpyAsync(&d, x.seg + x.m - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  SBD_CUDA(cudaStreamSynchronize(st));
+  x.distinct = (size_t)d;
+}
+
+void expand_space(sbdgpu_genop* g, const double* dW, double eps, int select, Expanded& x) {
+  if (!g->ready) throw Error{SBDGPU_ERR_STATE, "no operator: call sbdgpu_genop_set_terms first"};
+  switch (g->nw) {
+    case 1: expand_nw<1>(g, dW, eps, select, x); break;
+    case 2: expand_nw<2>(g, dW, eps, select, x); break;
+    default: expand_nw<4>(g, dW, eps, select, x); break;
+  }
+}
+
 }  // namespace
 
 namespace sbdgpu {
@@ -657,6 +853,46 @@ int sbdgpu_genop_davidson(sbdgpu_genop* g, const sbdgpu_opts* opts, double* W, d
     if (!opts || !W) throw Error{SBDGPU_ERR_ARG, "null argument"};
     if (!g->ready) throw Error{SBDGPU_ERR_STATE, "no operator: call sbdgpu_genop_set_terms first"};
     davidson(g, opts, W, energy, trace_e, trace_tol, max_trace, n_steps);
+  });
+}
+
+int sbdgpu_genop_ham_square(sbdgpu_genop* g, const double* W, double* res) {
+  return guarded(g, [&] {
+    if (!W || !res) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    cudaStream_t st = g->base.stream;
+    DevVecs v{{}, st};
+    double* dW = v.add(g->n);
+    SBD_CUDA(cudaMemcpyAsync(dW, W, sizeof(double) * g->n, cudaMemcpyHostToDevice, st));
+    Expanded x;
+    expand_space(g, dW, 0.0, 0, x);
+    double* sums = v.add(x.distinct);
+    SBD_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * x.distinct, st));
+    const unsigned gb = (unsigned)std::min<size_t>((x.m + 255) / 256 + 1, 148 * 8);
+    seg_sum_kernel<<<gb, 256, 0, st>>>(x.seg, x.idx, x.vals, sums, x.m);
+    SBD_CUDA(cudaGetLastError());
+    *res = sbdgpu::dot(&g->base, sums, sums, x.distinct);
+  });
+}
+
+int sbdgpu_genop_expand(sbdgpu_genop* g, const double* W, double eps_hb, uint64_t* out, size_t capacity,
+                        size_t* n_out) {
+  return guarded(g, [&] {
+    if (!W || !n_out) throw Error{SBDGPU_ERR_ARG, "null argument"};
+    cudaStream_t st = g->base.stream;
+    DevVecs v{{}, st};
+    double* dW = v.add(g->n);
+    SBD_CUDA(cudaMemcpyAsync(dW, W, sizeof(double) * g->n, cudaMemcpyHostToDevice, st));
+    Expanded x;
+    expand_space(g, dW, eps_hb, 1, x);
+    *n_out = x.distinct;
+    if (!out) return;
+    if (capacity < x.distinct) throw Error{SBDGPU_ERR_LIMIT, "output holds fewer states than the expanded basis"};
+    uint64_t* d = (uint64_t*)x.alloc(sizeof(uint64_t) * x.distinct * g->nw);
+    const unsigned gb = (unsigned)std::min<size_t>((x.m + 255) / 256 + 1, 148 * 8);
+    compact_kernel<<<gb, 256, 0, st>>>(x.keys, g->nw, x.idx, x.head, x.seg, d, x.m);
+    SBD_CUDA(cudaGetLastError());
+    SBD_CUDA(cudaMemcpyAsync(out, d, sizeof(uint64_t) * x.distinct * g->nw, cudaMemcpyDeviceToHost, st));
+    SBD_CUDA(cudaStreamSynchronize(st));
   });
 }
 

@@ -12,6 +12,7 @@
  *   GeneralOp_From_FCIDump                       out_of_place_func/stdmodel.h:13-98
  *   mult (W += H C)                              out_of_place_func/mult.h:268-291
  *   Lanczos (operator overload)                  out_of_place_func/lanczos.h:176-310
+ *   MeasHamSquare, ExpandBasis                   out_of_place_func/expand.h:10-366
  * and sbd::gpu::Davidson, a Davidson with on-the-fly sigma (an extension: the
  * reference's generic Davidson, out_of_place_func/davidson.h:19-196, runs on a
  * stored Hamiltonian).  One rank: communicators are accepted for signature
@@ -615,6 +616,25 @@ class DeviceOp {
     check(sbdgpu_genop_lanczos(g_, W.data(), max_it, eps, &e, n_iter), "sbdgpu_genop_lanczos");
     return e;
   }
+  // <W|H^2|W> over the expanded space (MeasHamSquare)
+  double ham_square(const std::vector<double>& W) {
+    double r = 0.0;
+    check(sbdgpu_genop_ham_square(g_, W.data(), &r), "sbdgpu_genop_ham_square");
+    return r;
+  }
+  // the expanded basis (ExpandBasis) as configurations of bit_length-bit words
+  std::vector<std::vector<size_t>> expand(const std::vector<double>& W, double eps_hb, size_t bit_length,
+                                          size_t words_out) {
+    size_t m = 0;
+    check(sbdgpu_genop_expand(g_, W.data(), eps_hb, nullptr, 0, &m), "sbdgpu_genop_expand");
+    std::vector<uint64_t> st(m * nw_);
+    check(sbdgpu_genop_expand(g_, W.data(), eps_hb, st.data(), m, &m), "sbdgpu_genop_expand");
+    std::vector<std::vector<size_t>> out(m, std::vector<size_t>(words_out, 0));
+    for (size_t i = 0; i < m; i++)
+      for (size_t q = 0; q < words_out * bit_length && q < 64 * (size_t)nw_; q++)
+        if ((st[i * nw_ + q / 64] >> (q % 64)) & 1ull) out[i][q / bit_length] |= size_t(1) << (q % bit_length);
+    return out;
+  }
   double davidson(std::vector<double>& W, int max_it, int max_nb, double eps, bool verbose = false) {
     sbdgpu_opts o{};
     o.max_it = max_it;
@@ -654,6 +674,26 @@ void mult(const GeneralOp<ElemT>& H, const std::vector<ElemT>& C, const Basis& B
   static_assert(std::is_same<ElemT, double>::value, "the B200 generic path runs in double");
   gpu::DeviceOp op(H, B, bit_length, sign);
   op.mult(C, W);
+}
+
+// <W|H^2|W> over every configuration H reaches from the basis
+// (expand.h:10-215), on one GPU
+template <typename ElemT>
+void MeasHamSquare(const GeneralOp<ElemT>& H, const Basis& B, const std::vector<ElemT>& W, size_t bit_length,
+                   MPI_Comm& /*comm*/, ElemT& res, bool sign) {
+  static_assert(std::is_same<ElemT, double>::value, "the B200 generic path runs in double");
+  gpu::DeviceOp op(H, B, bit_length, sign);
+  res = op.ham_square(W);
+}
+
+// The basis plus every configuration an off-diagonal term reaches from basis
+// state i with |coef * sign * W_i| > eps_hb (expand.h:217-366), on one GPU
+template <typename ElemT, typename RealT>
+void ExpandBasis(const GeneralOp<ElemT>& H, const Basis& B, const std::vector<ElemT>& W, Basis& Bnew, RealT eps_hb,
+                 size_t bit_length, MPI_Comm& comm, bool sign) {
+  static_assert(std::is_same<ElemT, double>::value, "the B200 generic path runs in double");
+  gpu::DeviceOp op(H, B, bit_length, sign);
+  Bnew.Init(op.expand(W, (double)eps_hb, bit_length, B.Config(0).size()), comm, true);
 }
 
 // Lanczos for the lowest eigenvalue (lanczos.h:176-310): W is the start

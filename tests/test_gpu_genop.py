@@ -140,6 +140,42 @@ def test_set_fcidump_equals_oracle_operator():
     g.close()
 
 
+@pytest.mark.parametrize("nw,sites", [(1, [0, 3, 5, 9, 12, 20, 33, 47, 50, 63]),
+                                      (2, [1, 17, 40, 62, 63, 64, 65, 90, 101, 127])])
+def test_ham_square_and_expand_match_oracle(nw, sites):
+    rng = np.random.default_rng(40 + nw)
+    ints, states = _basis(sites, 4, 0.6, rng, nw)  # many targets outside the basis
+    H = _operator(rng, sites, 30, 60, True)
+    W = rng.normal(size=len(ints))
+    W /= np.linalg.norm(W)
+    g = sbd_b200.GenOp(states, sign=True)
+    g.set_terms(*H)
+    ost = _oracle_states(ints, nw)
+    ref = G.ham_square(ost, H, W)
+    assert abs(g.ham_square(W) - ref) <= 1e-12 * ref
+    for eps in (0.0, 0.02):
+        got = g.expand(W, eps)
+        want = G.expand(ost, H, W, eps)
+        got_int = [sum(int(x) << (64 * k) for k, x in enumerate(row)) for row in got]
+        assert got_int == want
+    g.close()
+
+
+def test_ham_square_on_a_closed_space_is_the_norm_of_hw():
+    L, ne = 6, 2
+    _, H = _fcidump_op(L, ne, 23)
+    strs = synth.full_strings(L, ne)
+    states = np.array([int(a) | (int(b) << L) for a in strs for b in strs], dtype=np.uint64)
+    g = sbd_b200.GenOp(states, sign=True)
+    g.set_terms(*H)
+    W = np.random.default_rng(9).normal(size=len(states))
+    hw = g.mult(W)
+    # the full product space is closed under H: H^2 over the expanded space is |HW|^2
+    assert abs(g.ham_square(W) - hw @ hw) <= 1e-11 * (hw @ hw)
+    assert len(g.expand(W, 0.0)) == len(states)
+    g.close()
+
+
 def test_lanczos_matches_oracle():
     L, ne = 4, 2
     _, H = _fcidump_op(L, ne, 9)
@@ -168,3 +204,80 @@ def test_bad_input_is_refused():
     with pytest.raises(sbd_b200.SbdGpuError):
         g.set_terms([], [(1.0, [(True, 64), (False, 0)], 1)])  # site beyond one word
     g.close()
+
+
+CPP = r"""
+#include <cstdio>
+#include "sbd/sbd.h"
+// argv[1] FCIDUMP, argv[2] norb, argv[3] electrons per spin: full alpha x beta space,
+// bit_length 20 (the reference's default word width)
+int main(int argc, char** argv) {
+  const int L = std::atoi(argv[2]), ne = std::atoi(argv[3]);
+  const size_t bl = 20;
+  MPI_Comm comm = MPI_COMM_WORLD;
+  sbd::GeneralOp<double> H;
+  int norb = 0, nelec = 0;
+  sbd::GeneralOp_From_FCIDump(argv[1], comm, comm, norb, nelec, H);
+  std::vector<std::vector<size_t>> cfg;
+  for (uint64_t a = 0; a < (1ull << L); a++) {
+    if (__builtin_popcountll(a) != ne) continue;
+    for (uint64_t b = 0; b < (1ull << L); b++) {
+      if (__builtin_popcountll(b) != ne) continue;
+      const uint64_t x = a | (b << L);
+      std::vector<size_t> w((2 * L + bl - 1) / bl, 0);
+      for (int q = 0; q < 2 * L; q++)
+        if ((x >> q) & 1) w[q / bl] |= size_t(1) << (q % bl);
+      cfg.push_back(w);
+    }
+  }
+  sbd::Basis B(cfg, comm);
+  std::vector<double> W(B.Size(), 0.0);
+  W[0] = 1.0;
+  sbd::Lanczos(H, B, W, comm, 300, bl, 1, 1e-12, true);
+  double nrm = 0;
+  for (double x : W) nrm += x * x;
+  for (double& x : W) x /= std::sqrt(nrm);
+  std::vector<double> HW(B.Size(), 0.0);
+  sbd::mult(H, W, B, HW, bl, 1, comm, true);
+  double e = 0;
+  for (size_t i = 0; i < W.size(); i++) e += W[i] * HW[i];
+  double h2 = 0;
+  sbd::MeasHamSquare(H, B, W, bl, comm, h2, true);
+  sbd::Basis Bn;
+  sbd::ExpandBasis(H, B, W, Bn, 0.0, bl, comm, true);
+  std::printf("%zu %.15f %.15f %zu\n", B.Size(), e, h2, Bn.Size());
+  return 0;
+}
+"""
+
+
+def test_cpp_generic_path_on_the_gpu():
+    """A program written against the reference's generic API (FCIDUMP ->
+    GeneralOp, Basis of 20-bit words, Lanczos, mult, MeasHamSquare,
+    ExpandBasis) runs on the GPU through the drop-in header: its energy equals
+    the tpb Davidson energy, and at an eigenvector <H^2> = E^2 on the closed
+    full space, whose expansion adds nothing."""
+    import subprocess
+    from conftest import ROOT
+    L, ne = 5, 2
+    ints = synth.make_integrals(L, 31)
+    strs = synth.full_strings(L, ne)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs)
+    W0 = np.zeros(ctx.n)
+    W0[0] = 1.0
+    e_tpb, _, _, _ = ctx.davidson(W0, 200, 10, 1e-10)
+    ctx.close()
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "FCIDUMP")
+        synth.write_fcidump(p, ints, 2 * ne)
+        src, exe = os.path.join(td, "g.cc"), os.path.join(td, "g")
+        open(src, "w").write(CPP)
+        lib = os.path.join(ROOT, "sbd_b200")
+        subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(lib, "include"), "-I",
+                        os.path.join(ROOT, "include"), src, "-L", lib, "-lsbdgpu", f"-Wl,-rpath,{lib}", "-o", exe],
+                       check=True)
+        out = subprocess.run([exe, p, str(L), str(ne)], capture_output=True, text=True, check=True).stdout.split()
+    n, e, h2, n_new = int(out[0]), float(out[1]), float(out[2]), int(out[3])
+    assert n == len(strs) ** 2 and n_new == n
+    assert abs(e - e_tpb) < 1e-9
+    assert abs(h2 - e * e) < 1e-7 * e * e
