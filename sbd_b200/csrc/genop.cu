@@ -6,24 +6,27 @@
 // Layout in HBM:
 //   states      [n][nw] uint64 in the caller's order (site q at bit q%64 of
 //               word q/64), nw = 1, 2 or 4
-//   keys, perm  the states sorted (most significant word first) and, per
-//               sorted position, the caller's index: the target of every
-//               off-diagonal term is found by a branch-free binary search
+//   hash table  open addressing with linear probing over a power-of-two
+//               table of at least twice the states: key words and the
+//               caller's index (-1 marks an empty slot); the target of every
+//               off-diagonal term is found in one to three probes
 //   terms       the off-diagonal list as fixed-size records: annihilation and
 //               creation masks (the sites of the first n_dag operators and of
 //               the rest), the coefficient and the operator sites in order
-//               (for the fermionic sign); the diagonal list is folded into one
-//               number per state at set-up (hdiag)
+//               (for the fermionic sign), sorted by annihilation mask, with one
+//               bucket record per distinct mask; the diagonal list is folded
+//               into one number per state at set-up (hdiag)
 //
-// mult: one thread per bra state, the term records staged through shared
-// memory in chunks that every warp reads as broadcasts; a term applies when
-// its annihilated sites are occupied and its created sites empty after the
-// annihilation (two mask tests per word), which is the reference's sequential
-// test (mult.h:213-240) for terms whose annihilated sites are distinct and
-// whose created sites are distinct (a term that repeats a site in either part
-// never applies there and is dropped at set-up).  Each thread accumulates its
-// own W_i, so no atomics.  The work is integer and bound by the binary
-// searches' L2 reads, not by HBM.
+// mult: one warp per bra state.  The warp walks the buckets (warp-uniform),
+// skips every bucket whose annihilated sites are not all occupied in the
+// state, and splits the terms of the others over its lanes.  A term applies
+// when its created sites are empty after the annihilation, which with the
+// bucket's test is the reference's sequential test (mult.h:213-240) for terms
+// whose annihilated sites are distinct and whose created sites are distinct
+// (a term that repeats a site in either part never applies there and is
+// dropped at set-up).  The lanes' sums are reduced in the warp, so no
+// atomics.  For a chemistry operator a state's occupation admits about one
+// bucket in ten.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -44,9 +47,12 @@ struct sbdgpu_genop {
   size_t n = 0;
   int sign = 1;
   uint64_t* states = nullptr;
-  uint64_t* keys = nullptr;
-  int64_t* perm = nullptr;
-  void* terms = nullptr;       // off-diagonal records
+  uint64_t* hkeys = nullptr;  // hash table: [slots][nw] key words
+  int64_t* hidx = nullptr;    // [slots] caller index, -1 = empty
+  uint64_t hmask = 0;         // slots - 1
+  void* terms = nullptr;       // off-diagonal records, sorted by annihilation mask
+  void* buckets = nullptr;     // one record per distinct annihilation mask
+  size_t n_buckets = 0;
   size_t n_terms = 0;
   void* self_terms = nullptr;  // off-diagonal records that map a state onto itself
   size_t n_self = 0;
@@ -58,7 +64,6 @@ namespace {
 
 constexpr int kMaxOps = SBDGPU_GENOP_MAX_OPS;
 constexpr int kThreads = 256;
-constexpr int kChunk = 128;  // term records per shared-memory chunk
 
 template <int NW>
 struct Term {
@@ -76,34 +81,41 @@ struct DiagTerm {
 };
 
 template <int NW>
-__device__ __forceinline__ bool key_less(const uint64_t* a, const uint64_t* b) {
-#pragma unroll
-  for (int w = NW - 1; w >= 0; w--)
-    if (a[w] != b[w]) return a[w] < b[w];
-  return false;
+struct Bucket {
+  uint64_t ann[NW];
+  int64_t start, end;  // its terms in the sorted term array
+};
+
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
 }
 
-// sorted position of w, or -1
 template <int NW>
-__device__ __forceinline__ int64_t find_state(const uint64_t* __restrict__ keys, size_t n, const uint64_t* w) {
-  size_t lo = 0, len = n;
-  while (len > 0) {  // lower bound
-    size_t half = len >> 1;
-    uint64_t k[NW];
+__host__ __device__ __forceinline__ uint64_t hash_state(const uint64_t* w) {
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+  for (int x = 0; x < NW; x++) h = mix64(h ^ w[x]);
+  return h;
+}
+
+// caller index of state w, or -1
+template <int NW>
+__device__ __forceinline__ int64_t find_state(const uint64_t* __restrict__ hkeys, const int64_t* __restrict__ hidx,
+                                              uint64_t hmask, const uint64_t* w) {
+  uint64_t h = hash_state<NW>(w) & hmask;
+  for (;;) {  // the table is at most half full, so an empty slot ends every probe sequence
+    const int64_t id = __ldg(&hidx[h]);
+    if (id < 0) return -1;
+    bool eq = true;
 #pragma unroll
-    for (int x = 0; x < NW; x++) k[x] = __ldg(&keys[(lo + half) * NW + x]);
-    if (key_less<NW>(k, w)) {
-      lo += half + 1;
-      len -= half + 1;
-    } else {
-      len = half;
-    }
+    for (int x = 0; x < NW; x++) eq &= __ldg(&hkeys[h * NW + x]) == w[x];
+    if (eq) return id;
+    h = (h + 1) & hmask;
   }
-  if (lo >= n) return -1;
-#pragma unroll
-  for (int x = 0; x < NW; x++)
-    if (__ldg(&keys[lo * NW + x]) != w[x]) return -1;
-  return (int64_t)lo;
 }
 
 // parity of the occupied sites below q
@@ -149,45 +161,45 @@ __device__ __forceinline__ bool apply_term(const Term<NW>& t, const uint64_t* v,
   return true;
 }
 
-// W[i] += hdiag[i] C[i] + sum over off-diagonal terms of coef * sign * C[j]
+// W[i] += hdiag[i] C[i] + sum over off-diagonal terms of coef * sign * C[j]:
+// one warp per state, its lanes over the terms of each applicable bucket
+constexpr int kMultWarps = kThreads / 32;
 template <int NW>
-__global__ void __launch_bounds__(kThreads) mult_kernel(const uint64_t* __restrict__ states,
-                                                       const uint64_t* __restrict__ keys,
-                                                       const int64_t* __restrict__ perm, size_t n,
-                                                       const Term<NW>* __restrict__ terms, size_t n_terms, int sign,
+__global__ void __launch_bounds__(kThreads) mult_kernel(const uint64_t* __restrict__ states, size_t n,
+                                                       const uint64_t* __restrict__ hkeys,
+                                                       const int64_t* __restrict__ hidx, uint64_t hmask,
+                                                       const Bucket<NW>* __restrict__ buckets, size_t n_buckets,
+                                                       const Term<NW>* __restrict__ terms, int sign,
                                                        const double* __restrict__ hdiag,
                                                        const double* __restrict__ C, double* __restrict__ W) {
-  __shared__ Term<NW> sm[kChunk];
-  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
-  const bool live = i < n;
-  uint64_t v[NW];
-  double acc = 0.0;
-  if (live) {
+  const int lane = threadIdx.x & 31;
+  const size_t warps = (size_t)gridDim.x * kMultWarps;
+  for (size_t i = (size_t)blockIdx.x * kMultWarps + (threadIdx.x >> 5); i < n; i += warps) {
+    uint64_t v[NW];
 #pragma unroll
-    for (int x = 0; x < NW; x++) v[x] = states[i * NW + x];
-    acc = W[i] + hdiag[i] * C[i];
-  }
-  for (size_t t0 = 0; t0 < n_terms; t0 += kChunk) {
-    const int cnt = (int)min((size_t)kChunk, n_terms - t0);
-    __syncthreads();
-    {
-      // the chunk as 8-byte words
-      const uint64_t* src = reinterpret_cast<const uint64_t*>(terms + t0);
-      uint64_t* dst = reinterpret_cast<uint64_t*>(sm);
-      const int words = cnt * (int)(sizeof(Term<NW>) / 8);
-      for (int k = threadIdx.x; k < words; k += kThreads) dst[k] = src[k];
+    for (int x = 0; x < NW; x++) v[x] = __ldg(&states[i * NW + x]);
+    double acc = 0.0;
+    for (size_t b = 0; b < n_buckets; b++) {
+      bool ok = true;
+#pragma unroll
+      for (int x = 0; x < NW; x++) {
+        const uint64_t m = __ldg(&buckets[b].ann[x]);
+        ok &= (v[x] & m) == m;
+      }
+      if (!ok) continue;  // warp-uniform: the same state in every lane
+      const int64_t t1 = __ldg(&buckets[b].end);
+      for (int64_t t = __ldg(&buckets[b].start) + lane; t < t1; t += 32) {
+        uint64_t w[NW];
+        double s;
+        if (!apply_term<NW>(terms[t], v, sign, w, &s)) continue;
+        const int64_t j = find_state<NW>(hkeys, hidx, hmask, w);
+        if (j >= 0) acc += __ldg(&terms[t].coef) * s * __ldg(&C[j]);
+      }
     }
-    __syncthreads();
-    if (!live) continue;
-    for (int k = 0; k < cnt; k++) {
-      uint64_t w[NW];
-      double s;
-      if (!apply_term<NW>(sm[k], v, sign, w, &s)) continue;
-      const int64_t j = find_state<NW>(keys, n, w);
-      if (j >= 0) acc += sm[k].coef * s * __ldg(&C[__ldg(&perm[j])]);
-    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) W[i] = W[i] + hdiag[i] * C[i] + acc;
   }
-  if (live) W[i] = acc;
 }
 
 // hdiag[i] = sum of the diagonal terms whose sites are all occupied in state i
@@ -309,9 +321,25 @@ void set_terms_nw(sbdgpu_genop* g, size_t n_diag, const int64_t* diag_off, const
   }
   std::vector<Term<NW>> all, self;
   build_terms<NW>(NW, n_off, off_off, off_ops, off_ndag, off_coef, all, self);
+  // terms grouped by annihilation mask (stable), one bucket per mask
+  std::stable_sort(all.begin(), all.end(), [](const Term<NW>& a, const Term<NW>& b) {
+    return std::lexicographical_compare(a.ann, a.ann + NW, b.ann, b.ann + NW);
+  });
+  std::vector<Bucket<NW>> bk;
+  for (size_t t = 0; t < all.size(); t++) {
+    if (t == 0 || !std::equal(all[t].ann, all[t].ann + NW, all[t - 1].ann)) {
+      Bucket<NW> b;
+      std::memcpy(b.ann, all[t].ann, sizeof(b.ann));
+      b.start = (int64_t)t;
+      bk.push_back(b);
+    }
+    bk.back().end = (int64_t)t + 1;
+  }
   cudaFree(g->terms);
   cudaFree(g->self_terms);
-  g->terms = g->self_terms = nullptr;
+  cudaFree(g->buckets);
+  g->terms = g->self_terms = g->buckets = nullptr;
+  g->n_buckets = 0;
   g->ready = false;
   DiagTerm<NW>* d_dt = nullptr;
   try {
@@ -325,6 +353,8 @@ void set_terms_nw(sbdgpu_genop* g, size_t n_diag, const int64_t* diag_off, const
     if (!all.empty()) {
       g->terms = sbdgpu::dev_alloc(sizeof(Term<NW>) * all.size());
       SBD_CUDA(cudaMemcpyAsync(g->terms, all.data(), sizeof(Term<NW>) * all.size(), cudaMemcpyHostToDevice, st));
+      g->buckets = sbdgpu::dev_alloc(sizeof(Bucket<NW>) * bk.size());
+      SBD_CUDA(cudaMemcpyAsync(g->buckets, bk.data(), sizeof(Bucket<NW>) * bk.size(), cudaMemcpyHostToDevice, st));
     }
     if (!self.empty()) {
       g->self_terms = sbdgpu::dev_alloc(sizeof(Term<NW>) * self.size());
@@ -338,14 +368,18 @@ void set_terms_nw(sbdgpu_genop* g, size_t n_diag, const int64_t* diag_off, const
   }
   cudaFree(d_dt);
   g->n_terms = all.size();
+  g->n_buckets = bk.size();
   g->n_self = self.size();
   g->ready = true;
 }
 
 template <int NW>
 void mult_nw(sbdgpu_genop* g, const double* C, double* W) {
-  mult_kernel<NW><<<blocks_for(g->n), kThreads, 0, g->base.stream>>>(
-      g->states, g->keys, g->perm, g->n, static_cast<const Term<NW>*>(g->terms), g->n_terms, g->sign, g->hdiag, C, W);
+  const unsigned grid = (unsigned)std::min<size_t>((g->n + kMultWarps - 1) / kMultWarps, 148 * 16);
+  mult_kernel<NW><<<grid, kThreads, 0, g->base.stream>>>(g->states, g->n, g->hkeys, g->hidx, g->hmask,
+                                                        static_cast<const Bucket<NW>*>(g->buckets), g->n_buckets,
+                                                        static_cast<const Term<NW>*>(g->terms), g->sign, g->hdiag,
+                                                        C, W);
   SBD_CUDA(cudaGetLastError());
 }
 
@@ -748,29 +782,31 @@ int sbdgpu_genop_create(sbdgpu_genop** out, int device, int nwords, size_t nstat
     g->n = nstates;
     g->sign = sign ? 1 : 0;
     SBD_CUDA(cudaStreamCreateWithFlags(&g->base.stream, cudaStreamNonBlocking));
-    std::vector<int64_t> order(nstates);
-    std::iota(order.begin(), order.end(), 0);
-    auto less = [&](int64_t a, int64_t b) {
-      for (int w = nwords - 1; w >= 0; w--) {
-        const uint64_t x = states[a * nwords + w], y = states[b * nwords + w];
-        if (x != y) return x < y;
-      }
-      return false;
-    };
-    std::sort(order.begin(), order.end(), less);
-    std::vector<uint64_t> keys(nstates * nwords);
+    // the hash table: at least twice the states, a power of two
+    size_t slots = 1024;
+    while (slots < 2 * nstates) slots <<= 1;
+    std::vector<uint64_t> hk(slots * nwords, 0);
+    std::vector<int64_t> hi(slots, -1);
+    const uint64_t hmask = slots - 1;
     for (size_t i = 0; i < nstates; i++) {
-      if (i > 0 && !less(order[i - 1], order[i])) throw Error{SBDGPU_ERR_ARG, "repeated basis state"};
-      std::memcpy(&keys[i * nwords], &states[order[i] * nwords], sizeof(uint64_t) * nwords);
+      const uint64_t* w = &states[i * nwords];
+      uint64_t h = (nwords == 1 ? hash_state<1>(w) : nwords == 2 ? hash_state<2>(w) : hash_state<4>(w)) & hmask;
+      while (hi[h] >= 0) {
+        if (std::equal(w, w + nwords, &hk[h * nwords])) throw Error{SBDGPU_ERR_ARG, "repeated basis state"};
+        h = (h + 1) & hmask;
+      }
+      hi[h] = (int64_t)i;
+      std::memcpy(&hk[h * nwords], w, sizeof(uint64_t) * nwords);
     }
     const size_t bytes = sizeof(uint64_t) * nstates * nwords;
     g->states = (uint64_t*)sbdgpu::dev_alloc(bytes);
-    g->keys = (uint64_t*)sbdgpu::dev_alloc(bytes);
-    g->perm = (int64_t*)sbdgpu::dev_alloc(sizeof(int64_t) * nstates);
+    g->hkeys = (uint64_t*)sbdgpu::dev_alloc(sizeof(uint64_t) * hk.size());
+    g->hidx = (int64_t*)sbdgpu::dev_alloc(sizeof(int64_t) * slots);
+    g->hmask = hmask;
     SBD_CUDA(cudaMemcpyAsync(g->states, states, bytes, cudaMemcpyHostToDevice, g->base.stream));
-    SBD_CUDA(cudaMemcpyAsync(g->keys, keys.data(), bytes, cudaMemcpyHostToDevice, g->base.stream));
-    SBD_CUDA(cudaMemcpyAsync(g->perm, order.data(), sizeof(int64_t) * nstates, cudaMemcpyHostToDevice,
+    SBD_CUDA(cudaMemcpyAsync(g->hkeys, hk.data(), sizeof(uint64_t) * hk.size(), cudaMemcpyHostToDevice,
                              g->base.stream));
+    SBD_CUDA(cudaMemcpyAsync(g->hidx, hi.data(), sizeof(int64_t) * slots, cudaMemcpyHostToDevice, g->base.stream));
     SBD_CUDA(cudaStreamSynchronize(g->base.stream));
   });
   if (rc != SBDGPU_OK) {  // a bad argument, or no memory on the device
@@ -903,8 +939,9 @@ void sbdgpu_genop_destroy(sbdgpu_genop* g) {
   cudaSetDevice(g->base.device);
   if (g->base.stream) cudaStreamSynchronize(g->base.stream);
   cudaFree(g->states);
-  cudaFree(g->keys);
-  cudaFree(g->perm);
+  cudaFree(g->hkeys);
+  cudaFree(g->hidx);
+  cudaFree(g->buckets);
   cudaFree(g->terms);
   cudaFree(g->self_terms);
   cudaFree(g->hdiag);
