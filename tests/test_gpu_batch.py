@@ -63,12 +63,21 @@ def test_batch_step_counts_follow_single_runs():
         assert abs(s - len(te)) <= max(3, 0.1 * len(te)), (s, len(te))
 
 
+def _broken(n, seed):
+    # the closed-shell determinant plus a 1 % seeded random part: FP64 runs from
+    # the determinant alone stay in its spin-flip sector, FP32 rounding does not
+    w = np.random.default_rng(seed).normal(size=n)
+    w *= 0.01 / np.linalg.norm(w)
+    w[0] += 1.0
+    return w / np.linalg.norm(w)
+
+
 def test_batch_mixed_precision_runs_each_problem():
     ctxs, g = _contexts()
-    E, Ws, steps = sbd_b200.davidson_batch(ctxs[:3], [_unit(c.n) for c in ctxs[:3]], 300, 10, 1e-6,
-                                           precision=sbd_b200.MIXED)
-    for c, e in zip(ctxs[:3], E):
-        e1, _, _, _ = c.davidson(_unit(c.n), 300, 10, 1e-9)
+    W0 = [_broken(c.n, i) for i, c in enumerate(ctxs[:3])]
+    E, Ws, steps = sbd_b200.davidson_batch(ctxs[:3], W0, 300, 10, 1e-6, precision=sbd_b200.MIXED)
+    for c, w0, e in zip(ctxs[:3], W0, E):
+        e1, _, _, _ = c.davidson(w0, 300, 10, 1e-9)
         assert abs(e - e1) < 1e-8
 
 
