@@ -282,7 +282,8 @@ int sbdgpu_mlp_loss_grad(int device, const float* w, int B, const float* X, cons
  * singles per CTA (16, 8, 4, 2 or 1, where the integral block fits in shared
  * memory beside a row of C) and ab_threads threads per CTA (128, 256, 512 or
  * 1024); (0, 0) restores the default (the largest group that fits; 512
- * threads while two CTAs fit an SM, else 1024).  A shape that does not fit the
+ * threads while two CTAs fit an SM, else 1024, halved down to 128 while the
+ * warps outnumber the 32-string slices of beta strings).  A shape that does not fit the
  * basis is refused. */
 int sbdgpu_set_tuning(sbdgpu_ctx* ctx, int ab_group, int ab_threads);
 

@@ -323,10 +323,14 @@ void launch_ab_nt(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem, con
 }
 
 // threads per CTA: the tuned choice, else 512 while two CTAs fit an SM's
-// shared memory and 1024 when only one does
+// shared memory and 1024 when only one does, halved (down to 128) while the
+// warps would outnumber the 32-string slices of beta strings they loop over
 template <typename T, int G>
 void launch_ab(sbdgpu_ctx* c, const T* C, T* S, const T* vf, size_t smem, const AlphaSingles& as, int nt) {
-  if (nt == 0) nt = 2 * (smem + 1024) <= 228 * 1024 ? 512 : 1024;
+  if (nt == 0) {
+    nt = 2 * (smem + 1024) <= 228 * 1024 ? 512 : 1024;
+    while (nt > 128 && (size_t)(nt / 2) >= c->tab[1].nslice * 32) nt /= 2;
+  }
   switch (nt) {
     case 128: launch_ab_nt<T, G, 128>(c, C, S, vf, smem, as); break;
     case 256: launch_ab_nt<T, G, 256>(c, C, S, vf, smem, as); break;
