@@ -31,7 +31,7 @@ EXPORTS = [
     "sbdgpu_precond_train", "sbdgpu_precond_get", "sbdgpu_precond_set", "sbdgpu_precond_apply",
     "sbdgpu_mlp_loss_grad", "sbdgpu_genop_create", "sbdgpu_genop_set_terms", "sbdgpu_genop_mult",
     "sbdgpu_genop_mult_device", "sbdgpu_genop_diagonal", "sbdgpu_genop_lanczos", "sbdgpu_genop_davidson",
-    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy", "sbdgpu_genop_set_fcidump", "sbdgpu_set_tuning", "sbdgpu_genop_ham_square", "sbdgpu_genop_expand",
+    "sbdgpu_genop_last_error", "sbdgpu_genop_destroy", "sbdgpu_genop_set_fcidump", "sbdgpu_set_tuning", "sbdgpu_genop_ham_square", "sbdgpu_genop_expand", "sbdgpu_set_fp64_same_spin",
     "sbdgpu_autotune",
 ]
 
@@ -92,6 +92,7 @@ def lib():
         L.sbdgpu_mlp_loss_grad.argtypes = [ctypes.c_int, _fp, ctypes.c_int, _fp, _dp, _dp, _dp, _dp, _dp,
                                            ctypes.c_double, ctypes.c_double, _dp, _fp]
         L.sbdgpu_set_tuning.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+        L.sbdgpu_set_fp64_same_spin.argtypes = [_vp, ctypes.c_int]
         L.sbdgpu_autotune.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_float)]
         L.sbdgpu_store_hamiltonian.argtypes = [_vp, _u64p]
@@ -223,6 +224,11 @@ class Context:
         st = (ctypes.c_int * 2)()
         self._check(lib().sbdgpu_wait_selftest(self._h, int(spin_limit), st))
         return int(st[0]), int(st[1])
+
+    def set_fp64_same_spin(self, method: int) -> None:
+        """0: same-spin terms of the FP64 sigma as exact INT8 tensor-core
+        products where they fit; 1 (the default): the rows kernels."""
+        self._check(lib().sbdgpu_set_fp64_same_spin(self._h, int(method)))
 
     def set_tuning(self, ab_group: int, ab_threads: int) -> None:
         """Launch shape of the FP64 alpha-beta kernel ((0, 0): the default)."""

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsbdgpu.so")
-SOURCES = ["api.cu", "tables.cu", "sigma.cu", "misc.cu", "tc_ab.cu", "noalloc.cu", "stored.cu", "roots.cu", "batch.cu", "learned.cu", "gemm_same.cu", "genop.cu", "genop_fcidump.cu", "rdm.cu"]
+SOURCES = ["api.cu", "tables.cu", "sigma.cu", "misc.cu", "tc_ab.cu", "noalloc.cu", "stored.cu", "roots.cu", "batch.cu", "learned.cu", "gemm_same.cu", "genop.cu", "genop_fcidump.cu", "rdm.cu", "ozaki.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -756,6 +756,14 @@ int sbdgpu_precond_apply(sbdgpu_ctx* c, const double* Rh, double e0, double* out
   });
 }
 
+int sbdgpu_set_fp64_same_spin(sbdgpu_ctx* c, int method) {
+  return guarded(c, [&] {
+    if (method != 0 && method != 1) throw Error{SBDGPU_ERR_ARG, "method must be 0 or 1"};
+    SBD_CUDA(cudaStreamSynchronize(c->stream));
+    c->oz.mode = method;
+  });
+}
+
 const char* sbdgpu_last_error(sbdgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 void sbdgpu_destroy(sbdgpu_ctx* c) {
@@ -766,6 +774,7 @@ void sbdgpu_destroy(sbdgpu_ctx* c) {
   sbdgpu::free_learned(c);
   sbdgpu::free_dense_same(c);
   sbdgpu::free_rdm_tables(c);
+  sbdgpu::free_ozaki(c);
   sbdgpu::free_tables(c->tab[0]);
   sbdgpu::free_tables(c->tab[1]);
   cudaFree(c->astr); cudaFree(c->bstr); cudaFree(c->h1); cudaFree(c->vf); cudaFree(c->ja); cudaFree(c->jb);

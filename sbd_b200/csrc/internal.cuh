@@ -105,6 +105,18 @@ struct sbdgpu_ctx {
   int blk_max = 0;
   size_t blk_r0 = 0, blk_r1 = 0;
   sbdgpu::SpinTables tab[2];
+  // same-spin terms of the FP64 sigma on the integer tensor cores (ozaki.cu)
+  struct {
+    int mode = 1;          // 0 automatic, 1 the rows kernels only (the default until measured)
+    bool ready = false, failed = false;
+    int8_t* h0r[2] = {nullptr, nullptr};  // residues of the string-only operators
+    int* h0e[2] = {nullptr, nullptr};     // their row exponents
+    int8_t* cr = nullptr;                 // residues of C (row-scaled)
+    int8_t* ctr = nullptr;                // residues of C^T (row-scaled)
+    int* ce = nullptr;
+    int* cte = nullptr;
+    int32_t* prod = nullptr;              // INT8 products, one per prime
+  } oz;
   // alpha-beta launch shape of the FP64 sigma (0: the shared-memory heuristic)
   int ab_group = 0, ab_threads = 0;
   // RDM tables: beta singles grouped by excitation, bra row of every alpha single
@@ -171,6 +183,11 @@ void ensure_rdm_tables(sbdgpu_ctx* c);
 void free_rdm_tables(sbdgpu_ctx* c);
 // sigma.cu: the alpha-beta launch shapes (group size, threads) open to this context's FP64 sigma
 std::vector<std::pair<int, int>> ab_shapes(sbdgpu_ctx* c);
+// ozaki.cu: the FP64 same-spin terms as exact INT8 products
+bool ensure_ozaki(sbdgpu_ctx* c);
+void free_ozaki(sbdgpu_ctx* c);
+bool use_ozaki(sbdgpu_ctx* c);
+bool same_spin_ozaki_fp64(sbdgpu_ctx* c, const double* C, double* S, double* ct, double* st, bool events);
 // genop.cu: record an error message on a generic-path object
 void genop_set_error(sbdgpu_genop* g, const std::string& msg);
 void occupation(sbdgpu_ctx* c, const double* dW, double* dens);

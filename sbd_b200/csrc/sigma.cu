@@ -443,6 +443,12 @@ void sigma_fp64(sbdgpu_ctx* c, const double* C, double* S) {
     return;
   }
   ensure_scratch(c);
+  if (use_ozaki(c) && same_spin_ozaki_fp64(c, C, S, c->ct, c->st, true)) {
+    const SpinTables& ta = c->tab[0];
+    alpha_beta<double>(c, C, S, c->vf, AlphaSingles{ta.s_off, ta.s_idx, ta.s_info, ta.max_s, 0});
+    SBD_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    return;
+  }
   sigma_launch<double>(c, C, S, c->ct, c->st, c->ja, c->jb, c->vf, true);
 }
 

@@ -80,3 +80,31 @@ def test_mixed_sigma_dense_same_spin(norb, ne, count, seed):
     e64, _, _, _ = ctx.davidson(W0, 200, 10, 1e-7)
     e32, _, _, tt = ctx.davidson(W0, 200, 10, 1e-4, precision=sbd_b200.MIXED, restart_keep=3, restart_prev=1)
     assert tt[-1] < 1e-4 and abs(e32 - e64) < 1e-6
+
+
+@pytest.mark.parametrize("norb,ne,count,seed", [(16, 5, 1100, 31), (18, 4, 1500, 32), (16, 5, 1102, 33)])
+def test_fp64_same_spin_integer_products(norb, ne, count, seed):
+    """From 1,024 strings per spin (multiples of 4) the FP64 sigma forms its
+    same-spin terms as exact INT8 tensor-core products (residues modulo 15
+    primes, CRT): equal to the rows kernels to FP64 rounding, for normalised
+    and unnormalised vectors; 1,102 strings keep the rows kernels."""
+    import sbd_b200
+    from sbd_b200 import synth
+    from conftest import seeded_vector
+    ints, ne, strs = synth.make_small(norb, ne, count, seed)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs)
+    C = seeded_vector(ctx.n, seed)
+    ctx.set_fp64_same_spin(1)
+    ref = ctx.sigma(C)
+    ctx.set_fp64_same_spin(0)
+    got = ctx.sigma(C)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    C2 = C * np.exp(np.random.default_rng(seed).normal(size=ctx.n) * 4)  # wide dynamic range
+    ctx.set_fp64_same_spin(1)
+    ref2 = ctx.sigma(C2)
+    ctx.set_fp64_same_spin(0)
+    got2 = ctx.sigma(C2)
+    assert np.abs(got2 - ref2).max() <= 1e-12 * np.abs(ref2).max()
+    with pytest.raises(sbd_b200.SbdGpuError):
+        ctx.set_fp64_same_spin(2)
+    ctx.close()
