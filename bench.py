@@ -617,6 +617,7 @@ def run_gpu(args):
         pg = dist
     ints, ne, strs = synth.make_workload(args.workload, seed=0)
     ctx = sbd_b200.context_from_integrals(ints, strs, strs, device=dev)
+    ctx.set_fp64_same_spin(args.fp64_same_spin)
     st = table_stats(ctx)
     alg = algorithmic(ctx, st)
     n = ctx.n
@@ -774,6 +775,8 @@ def main():
     ap.add_argument("--learn-steps", type=int, default=600, help="Adam steps of the learned preconditioner")
     ap.add_argument("--rdm", action="store_true", help="also time the 1/2-RDMs")
     ap.add_argument("--genop", action="store_true", help="also time the generic second-quantised path")
+    ap.add_argument("--fp64-same-spin", type=int, default=1,
+                    help="FP64 same-spin terms: 0 = exact INT8 tensor-core products, 1 = rows kernels")
     ap.add_argument("--rdm-workload", default="c1_L26_6e_4000", help="workload of the RDM block")
     ap.add_argument("--config4", action="store_true",
                     help="also run the 400M-determinant workload (norb 48, 10a/10b, 20,000 strings)")
