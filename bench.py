@@ -39,6 +39,10 @@ UNIT = "sigma/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 LAUNCHES_PER_SIGMA = 7  # phase, rows(alpha), transpose, rows(beta), transpose-add, alpha-beta, phase
+# with the same-spin terms as INT8 products: phase, transpose, 2 row exponents,
+# 2 residue passes, 2 singles-Coulomb kernels, 2 CRT reconstructions,
+# transpose-add, alpha-beta, phase (the 30 INT8 GEMMs are cuBLAS's)
+LAUNCHES_PER_SIGMA_INT8 = 13
 
 
 def dist_env():
@@ -701,7 +705,8 @@ def run_gpu(args):
                    "l2": "inputs (1.15 GB per vector) larger than L2; no flush"},
         "e2e": {"value": world * 1000.0 / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
-        "gpu_launches": LAUNCHES_PER_SIGMA * args.steps * 2,
+        "gpu_launches": (LAUNCHES_PER_SIGMA_INT8 if args.fp64_same_spin == 0 and min(ctx.na, ctx.nb) >= 1024
+                         and ctx.na % 4 == 0 and ctx.nb % 4 == 0 else LAUNCHES_PER_SIGMA) * args.steps * 2,
         "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": achieved, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved / hbm_peak, "peak_source": peak_kind,
                      "traffic": traffic,
@@ -775,7 +780,7 @@ def main():
     ap.add_argument("--learn-steps", type=int, default=600, help="Adam steps of the learned preconditioner")
     ap.add_argument("--rdm", action="store_true", help="also time the 1/2-RDMs")
     ap.add_argument("--genop", action="store_true", help="also time the generic second-quantised path")
-    ap.add_argument("--fp64-same-spin", type=int, default=1,
+    ap.add_argument("--fp64-same-spin", type=int, default=0,
                     help="FP64 same-spin terms: 0 = exact INT8 tensor-core products, 1 = rows kernels")
     ap.add_argument("--rdm-workload", default="c1_L26_6e_4000", help="workload of the RDM block")
     ap.add_argument("--config4", action="store_true",

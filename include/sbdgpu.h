@@ -292,12 +292,12 @@ int sbdgpu_set_tuning(sbdgpu_ctx* ctx, int ab_group, int ab_threads);
  * in *ab_group, *ab_threads, *best_ms (each may be NULL). */
 int sbdgpu_autotune(sbdgpu_ctx* ctx, int reps, int* ab_group, int* ab_threads, float* best_ms);
 
-/* How the FP64 sigma forms its same-spin terms (an extension): method 0 =
- * as exact INT8 tensor-core products of the dense string-only
+/* How the FP64 sigma forms its same-spin terms (an extension): method 0 (the
+ * default) = as exact INT8 tensor-core products of the dense string-only
  * operator (residues modulo 15 primes, CRT reconstruction; FP64-accurate: the
  * scaled operands are rounded to 49-bit integers) where both spins have at
  * least 1,024 strings (multiples of 4) and the residues fit in device memory,
- * else the rows kernels; method 1 (the default) = the rows kernels always. */
+ * else the rows kernels; method 1 = the rows kernels always. */
 int sbdgpu_set_fp64_same_spin(sbdgpu_ctx* ctx, int method);
 
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);

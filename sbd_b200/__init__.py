@@ -226,8 +226,8 @@ class Context:
         return int(st[0]), int(st[1])
 
     def set_fp64_same_spin(self, method: int) -> None:
-        """0: same-spin terms of the FP64 sigma as exact INT8 tensor-core
-        products where they fit; 1 (the default): the rows kernels."""
+        """0 (the default): same-spin terms of the FP64 sigma as exact INT8
+        tensor-core products where they fit; 1: the rows kernels."""
         self._check(lib().sbdgpu_set_fp64_same_spin(self._h, int(method)))
 
     def set_tuning(self, ab_group: int, ab_threads: int) -> None:

@@ -107,7 +107,7 @@ struct sbdgpu_ctx {
   sbdgpu::SpinTables tab[2];
   // same-spin terms of the FP64 sigma on the integer tensor cores (ozaki.cu)
   struct {
-    int mode = 1;          // 0 automatic, 1 the rows kernels only (the default until measured)
+    int mode = 0;          // 0 automatic (the default), 1 the rows kernels only
     bool ready = false, failed = false;
     int8_t* h0r[2] = {nullptr, nullptr};  // residues of the string-only operators
     int* h0e[2] = {nullptr, nullptr};     // their row exponents
