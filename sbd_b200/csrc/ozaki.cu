@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <utility>
 
 #include "internal.cuh"
 
@@ -35,20 +36,43 @@ namespace {
 
 constexpr int kMods = 15;
 constexpr int kBits = 49;
+constexpr int kMaxExp = 1000;  // 2^kMaxExp and 2^-(kMaxExp - kBits) are normal doubles
 constexpr int kT = 256;
-const int kPrimes[kMods] = {251, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193, 191, 181, 179, 173};
 
-__constant__ int c_mod[kMods];
-__constant__ unsigned long long c_wlo[kMods], c_whi[kMods];  // CRT weights, < M
-__constant__ unsigned long long c_Mlo, c_Mhi;                 // M
-__constant__ double c_Mdbl;
+// the primes, as compile-time constants wherever the index is one (the
+// compiler then reduces by multiply-high and shift, not by a division)
+__host__ __device__ constexpr unsigned prime_at(int l) {
+  return l == 0 ? 251u : l == 1 ? 241u : l == 2 ? 239u : l == 3 ? 233u : l == 4 ? 229u : l == 5 ? 227u
+       : l == 6 ? 223u : l == 7 ? 211u : l == 8 ? 199u : l == 9 ? 197u : l == 10 ? 193u : l == 11 ? 191u
+       : l == 12 ? 181u : l == 13 ? 179u : 173u;
+}
+__host__ __device__ constexpr unsigned pow2_mod(int k, unsigned m) {
+  unsigned r = 1;
+  for (int i = 0; i < k; i++) r = (2 * r) % m;
+  return r;
+}
+template <int L>
+struct PrimeK {
+  static constexpr unsigned m = prime_at(L);
+  static constexpr unsigned p25 = pow2_mod(25, m);      // 2^25 mod m
+  static constexpr unsigned off49 = m - pow2_mod(49, m);  // -2^49 mod m, in [1, m]
+};
 
-// exponent that scales a row (or column) with maximum |x| to below 2^kBits
+__constant__ unsigned c_w[kMods][4];          // CRT weights (< M) in 32-bit limbs, lowest first
+__constant__ unsigned long long c_Mlo, c_Mhi;  // M
+__constant__ double c_Minv;                    // 1 / M
+
+// 2^k for -1022 <= k <= 1023, from its bit pattern
+__device__ __forceinline__ double pow2(int k) { return __longlong_as_double((long long)(k + 1023) << 52); }
+
+// exponent that scales a row (or column) with maximum |x| to below 2^kBits;
+// at most kMaxExp, so that 2^e is a normal double (rows below 2^-951 keep
+// fewer bits)
 __device__ __forceinline__ int scale_exp(double amax) {
   if (!(amax > 0.0)) return 0;
   int ex;
   frexp(amax, &ex);  // amax = f * 2^ex, f in [0.5, 1)
-  return kBits - ex;
+  return min(kBits - ex, kMaxExp);
 }
 
 // per-row exponent of a row-major [rows][cols] matrix
@@ -66,44 +90,93 @@ __global__ void __launch_bounds__(kT) row_exp_kernel(const double* __restrict__ 
   }
 }
 
-// symmetric residues modulo the primes of round(X * 2^e_row), int8, [kMods][rows*cols]
+// The symmetric residue modulo prime L of y = hu 2^25 + lo - 2^49 (an
+// integer of magnitude below 2^49 split so that every step is 32-bit).
+template <int L>
+__device__ __forceinline__ unsigned sym_residue_byte(unsigned hu, unsigned lo) {
+  constexpr unsigned m = PrimeK<L>::m;
+  const unsigned t = (hu % m) * PrimeK<L>::p25 + lo % m + PrimeK<L>::off49;  // < 2^17, = y mod m
+  const int r = (int)(t % m);
+  return (unsigned)(uint8_t)(int8_t)(r > (int)(m / 2) ? r - (int)m : r);
+}
+
+template <int L>
+__device__ __forceinline__ void store_residues4(const unsigned (&hu)[4], const unsigned (&lo)[4], int8_t* out,
+                                                size_t n, size_t at) {
+  const unsigned packed = sym_residue_byte<L>(hu[0], lo[0]) | sym_residue_byte<L>(hu[1], lo[1]) << 8 |
+                          sym_residue_byte<L>(hu[2], lo[2]) << 16 | sym_residue_byte<L>(hu[3], lo[3]) << 24;
+  *reinterpret_cast<unsigned*>(out + (size_t)L * n + at) = packed;
+}
+
+template <size_t... L>
+__device__ __forceinline__ void store_all_residues(std::index_sequence<L...>, const unsigned (&hu)[4],
+                                                   const unsigned (&lo)[4], int8_t* out, size_t n, size_t at) {
+  (store_residues4<(int)L>(hu, lo, out, n, at), ...);
+}
+
+// symmetric residues modulo the primes of round(X * 2^e_row), int8,
+// [kMods][rows*cols]; one block per row, four consecutive entries per thread
+// (cols a multiple of 4)
 __global__ void __launch_bounds__(kT) residue_kernel(const double* __restrict__ X, size_t rows, size_t cols,
                                                     const int* __restrict__ e, int8_t* __restrict__ out) {
-  const size_t n = rows * cols;
-  for (size_t i = (size_t)blockIdx.x * kT + threadIdx.x; i < n; i += (size_t)gridDim.x * kT) {
-    const double y = rint(ldexp(X[i], e[i / cols]));  // an integer, |y| < 2^kBits: exact in FP64
+  const size_t n = rows * cols, row = blockIdx.x;
+  const double scale = pow2(e[row]);  // e <= kMaxExp; >= kBits - 1024
+  const double* xr = X + row * cols;
+  for (size_t c = 4 * (size_t)threadIdx.x; c < cols; c += 4 * kT) {
+    const double2 x01 = *reinterpret_cast<const double2*>(xr + c);
+    const double2 x23 = *reinterpret_cast<const double2*>(xr + c + 2);
+    const double x[4] = {x01.x, x01.y, x23.x, x23.y};
+    unsigned hu[4], lo[4];
 #pragma unroll
-    for (int l = 0; l < kMods; l++) {
-      const double m = (double)c_mod[l];
-      double r = y - m * floor(y / m);  // m * floor(...) < 2^kBits: exact
-      if (r < 0.0) r += m;
-      if (r >= m) r -= m;
-      int ri = (int)r;
-      if (ri > c_mod[l] / 2) ri -= c_mod[l];
-      out[(size_t)l * n + i] = (int8_t)ri;
+    for (int j = 0; j < 4; j++) {
+      const long long y = __double2ll_rn(x[j] * scale);  // |y| < 2^kBits: the scaling is exact
+      hu[j] = (unsigned)((y >> 25) + (1LL << 24));     // in [0, 2^25)
+      lo[j] = (unsigned)(y & 0x1FFFFFFLL);
     }
+    store_all_residues(std::make_index_sequence<kMods>{}, hu, lo, out, n, row * cols + c);
   }
 }
 
-// S[i] += (integer product, from its residues) * 2^-(e_row + e_col)
+template <int L>
+__device__ __forceinline__ void crt_term(const int32_t* __restrict__ P, size_t n, size_t i,
+                                         unsigned long long (&a)[4]) {
+  constexpr int m = (int)PrimeK<L>::m;
+  int r = __ldg(&P[(size_t)L * n + i]) % m;
+  r += r < 0 ? m : 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) a[q] += (unsigned long long)c_w[L][q] * (unsigned)r;  // < 2^44 in all
+}
+
+template <size_t... L>
+__device__ __forceinline__ void crt_all(std::index_sequence<L...>, const int32_t* __restrict__ P, size_t n, size_t i,
+                                        unsigned long long (&a)[4]) {
+  (crt_term<(int)L>(P, n, i, a), ...);
+}
+
+__device__ __forceinline__ double u128_to_double(unsigned __int128 x) {
+  return (double)(unsigned long long)(x >> 64) * 18446744073709551616.0 + (double)(unsigned long long)x;
+}
+
+// S[row][col] += (integer product, from its residues) * 2^-(e_row + e_col);
+// one block per row
 __global__ void __launch_bounds__(kT) crt_add_kernel(const int32_t* __restrict__ P, size_t rows, size_t cols,
                                                     const int* __restrict__ e_row, const int* __restrict__ e_col,
                                                     double* __restrict__ S) {
-  const size_t n = rows * cols;
-  for (size_t i = (size_t)blockIdx.x * kT + threadIdx.x; i < n; i += (size_t)gridDim.x * kT) {
-    unsigned __int128 acc = 0;
-#pragma unroll
-    for (int l = 0; l < kMods; l++) {
-      int r = P[(size_t)l * n + i] % c_mod[l];
-      if (r < 0) r += c_mod[l];
-      const unsigned __int128 w = ((unsigned __int128)c_whi[l] << 64) | c_wlo[l];
-      acc += w * (unsigned)r;  // < kMods * 251 * M < 2^128
-    }
-    const unsigned __int128 M = ((unsigned __int128)c_Mhi << 64) | c_Mlo;
+  const size_t n = rows * cols, row = blockIdx.x;
+  const int er = e_row[row];
+  const unsigned __int128 M = ((unsigned __int128)c_Mhi << 64) | c_Mlo;
+  for (size_t c = threadIdx.x; c < cols; c += kT) {
+    const size_t i = row * cols + c;
+    unsigned long long a[4] = {0, 0, 0, 0};
+    crt_all(std::make_index_sequence<kMods>{}, P, n, i, a);
+    // carries: acc = sum_l r_l w_l < kMods * 251 * M < 2^128
+    a[1] += a[0] >> 32;
+    a[2] += a[1] >> 32;
+    a[3] += a[2] >> 32;
+    const unsigned __int128 acc = ((unsigned __int128)a[3] << 96) | ((unsigned __int128)(a[2] & 0xFFFFFFFFull) << 64) |
+                                  ((unsigned __int128)(a[1] & 0xFFFFFFFFull) << 32) | (a[0] & 0xFFFFFFFFull);
     // acc mod M: the quotient is below 2^12; estimate it in FP64, then correct
-    const double accd = (double)(unsigned long long)(acc >> 64) * 18446744073709551616.0 +
-                        (double)(unsigned long long)acc;
-    unsigned long long q = (unsigned long long)(accd / c_Mdbl);
+    unsigned long long q = (unsigned long long)(u128_to_double(acc) * c_Minv);
     unsigned __int128 qm = M * q;
     while (qm > acc) {
       qm -= M;
@@ -111,18 +184,11 @@ __global__ void __launch_bounds__(kT) crt_add_kernel(const int32_t* __restrict__
     }
     unsigned __int128 x = acc - qm;
     while (x >= M) x -= M;
-    double v;
-    if (x > (M >> 1)) {  // negative: x - M
-      const unsigned __int128 y = M - x;
-      v = -((double)(unsigned long long)(y >> 64) * 18446744073709551616.0 + (double)(unsigned long long)y);
-    } else {
-      v = (double)(unsigned long long)(x >> 64) * 18446744073709551616.0 + (double)(unsigned long long)x;
-    }
-    S[i] += ldexp(v, -(e_row[i / cols] + e_col[i % cols]));
+    const double v = x > (M >> 1) ? -u128_to_double(M - x) : u128_to_double(x);  // the symmetric representative
+    const int s = -(er + e_col[c]);
+    S[i] += (s >= -1022 && s <= 1023) ? v * pow2(s) : ldexp(v, s);
   }
 }
-
-unsigned grid_of(size_t n) { return (unsigned)std::min<size_t>((n + kT - 1) / kT, 148 * 8); }
 
 // the string-only same-spin operator of one spin, dense FP64 [n][n]
 __global__ void __launch_bounds__(kT) dense_h0_kernel(size_t n, const int64_t* __restrict__ s_off,
@@ -139,7 +205,8 @@ __global__ void __launch_bounds__(kT) dense_h0_kernel(size_t n, const int64_t* _
   for (int64_t k = d_off[row] + threadIdx.x; k < d_off[row + 1]; k += kT) Hr[d_idx[k]] = d_val[k];
 }
 
-// S[row][col] (=) [hii C] + sum over the bra's singles of s J_pq[col] C[ket][col] (FP64)
+// S[row][col] (=) [hii C] + sum over the bra's singles of s J_pq[col] C[ket][col] (FP64);
+// two consecutive columns per thread (ncols even)
 template <bool kWithDiag>
 __global__ void __launch_bounds__(kT) jsingles64_kernel(const double* __restrict__ C, double* __restrict__ S,
                                                        size_t ncols, const double* __restrict__ hii,
@@ -148,41 +215,48 @@ __global__ void __launch_bounds__(kT) jsingles64_kernel(const double* __restrict
                                                        const uint32_t* __restrict__ s_info,
                                                        const double* __restrict__ J) {
   const size_t row = blockIdx.x;
-  const size_t col = (size_t)blockIdx.y * kT + threadIdx.x;
+  const size_t col = 2 * ((size_t)blockIdx.y * kT + threadIdx.x);
   if (col >= ncols) return;
-  double acc = kWithDiag ? hii[row * ncols + col] * C[row * ncols + col] : 0.0;
-  for (int64_t k = s_off[row]; k < s_off[row + 1]; k++) {
+  double2 acc = {0.0, 0.0};
+  if (kWithDiag) {
+    const double2 h = *reinterpret_cast<const double2*>(hii + row * ncols + col);
+    const double2 x = *reinterpret_cast<const double2*>(C + row * ncols + col);
+    acc = {h.x * x.x, h.y * x.y};
+  }
+  const int64_t k1 = s_off[row + 1];
+#pragma unroll 4
+  for (int64_t k = s_off[row]; k < k1; k++) {
     const size_t j = (size_t)__ldg(&s_idx[k]);
     const uint32_t info = __ldg(&s_info[k]);
-    const double jv = __ldg(&J[(size_t)((info >> 12) & 0xFFFu) * ncols + col]);
-    acc += ((info & 0x80000000u) ? -jv : jv) * __ldg(&C[j * ncols + col]);
+    const double2 jv = __ldg(reinterpret_cast<const double2*>(J + (size_t)((info >> 12) & 0xFFFu) * ncols + col));
+    const double2 x = __ldg(reinterpret_cast<const double2*>(C + j * ncols + col));
+    const double sg = (info & 0x80000000u) ? -1.0 : 1.0;
+    acc.x = fma(sg * jv.x, x.x, acc.x);
+    acc.y = fma(sg * jv.y, x.y, acc.y);
   }
-  S[row * ncols + col] = acc;
+  *reinterpret_cast<double2*>(S + row * ncols + col) = acc;
 }
 
 // the CRT constants in constant memory on the current device
 void upload_crt_constants() {
   unsigned __int128 M = 1;
-  for (int l = 0; l < kMods; l++) M *= (unsigned)kPrimes[l];
-  unsigned long long wlo[kMods], whi[kMods];
+  for (int l = 0; l < kMods; l++) M *= prime_at(l);
+  unsigned w32[kMods][4];
   for (int l = 0; l < kMods; l++) {
-    const unsigned m = (unsigned)kPrimes[l];
+    const unsigned m = prime_at(l);
     const unsigned __int128 Ml = M / m;
     const unsigned r = (unsigned)(Ml % m);
     unsigned inv = 1;
     while ((unsigned long long)r * inv % m != 1) inv++;  // m < 256
     const unsigned __int128 w = (Ml * inv) % M;  // Ml * inv < M * 256 < 2^124
-    wlo[l] = (unsigned long long)w;
-    whi[l] = (unsigned long long)(w >> 64);
+    for (int q = 0; q < 4; q++) w32[l][q] = (unsigned)(w >> (32 * q));
   }
   const unsigned long long mlo = (unsigned long long)M, mhi = (unsigned long long)(M >> 64);
-  const double md = (double)mhi * 18446744073709551616.0 + (double)mlo;
-  SBD_CUDA(cudaMemcpyToSymbol(c_mod, kPrimes, sizeof(kPrimes)));
-  SBD_CUDA(cudaMemcpyToSymbol(c_wlo, wlo, sizeof(wlo)));
-  SBD_CUDA(cudaMemcpyToSymbol(c_whi, whi, sizeof(whi)));
+  const double minv = 1.0 / ((double)mhi * 18446744073709551616.0 + (double)mlo);
+  SBD_CUDA(cudaMemcpyToSymbol(c_w, w32, sizeof(w32)));
   SBD_CUDA(cudaMemcpyToSymbol(c_Mlo, &mlo, sizeof(mlo)));
   SBD_CUDA(cudaMemcpyToSymbol(c_Mhi, &mhi, sizeof(mhi)));
-  SBD_CUDA(cudaMemcpyToSymbol(c_Mdbl, &md, sizeof(md)));
+  SBD_CUDA(cudaMemcpyToSymbol(c_Minv, &minv, sizeof(minv)));
 }
 
 // INT8 GEMM, column-major: out (m x n, int32) = op(A) op(B); false when
@@ -224,7 +298,7 @@ bool ensure_ozaki(sbdgpu_ctx* c) {
       c->oz.h0e[spin] = (int*)dev_alloc(sizeof(int) * n);
       row_exp_kernel<<<(unsigned)n, kT, 0, st>>>(tmp, n, c->oz.h0e[spin]);
       c->oz.h0r[spin] = (int8_t*)dev_alloc((size_t)kMods * n * n);
-      residue_kernel<<<grid_of(n * n), kT, 0, st>>>(tmp, n, n, c->oz.h0e[spin], c->oz.h0r[spin]);
+      residue_kernel<<<(unsigned)n, kT, 0, st>>>(tmp, n, n, c->oz.h0e[spin], c->oz.h0r[spin]);
       SBD_CUDA(cudaGetLastError());
       SBD_CUDA(cudaStreamSynchronize(st));
     }
@@ -285,14 +359,15 @@ bool same_spin_ozaki_fp64(sbdgpu_ctx* c, const double* C, double* S, double* ct,
   const SpinTables& ta = c->tab[0];
   const SpinTables& tb = c->tab[1];
   cublasHandle_t h = static_cast<cublasHandle_t>(c->blas);
+  if (((uintptr_t)C | (uintptr_t)S) & 15) return false;  // the kernels move pairs of doubles
   SBD_CUDA(cudaGetLastError());
   if (events) SBD_CUDA(cudaEventRecord(c->ev[0], s));
   // scaled residues of C (rows: for the beta product) and of C^T (for the alpha product)
   transpose(C, ct, na, nb, s);
   row_exp_kernel<<<(unsigned)na, kT, 0, s>>>(C, nb, c->oz.ce);
   row_exp_kernel<<<(unsigned)nb, kT, 0, s>>>(ct, na, c->oz.cte);
-  residue_kernel<<<grid_of(N), kT, 0, s>>>(C, na, nb, c->oz.ce, c->oz.cr);
-  residue_kernel<<<grid_of(N), kT, 0, s>>>(ct, nb, na, c->oz.cte, c->oz.ctr);
+  residue_kernel<<<(unsigned)na, kT, 0, s>>>(C, na, nb, c->oz.ce, c->oz.cr);
+  residue_kernel<<<(unsigned)nb, kT, 0, s>>>(ct, nb, na, c->oz.cte, c->oz.ctr);
   SBD_CUDA(cudaGetLastError());
   // alpha: sigma^T (nb x na, column-major) = (C^T)(H0a^T), one INT8 product per prime
   for (int l = 0; l < kMods; l++)
@@ -301,9 +376,9 @@ bool same_spin_ozaki_fp64(sbdgpu_ctx* c, const double* C, double* S, double* ct,
       c->oz.failed = true;
       return false;
     }
-  jsingles64_kernel<true><<<dim3((unsigned)na, (unsigned)((nb + kT - 1) / kT)), kT, 0, s>>>(
+  jsingles64_kernel<true><<<dim3((unsigned)na, (unsigned)((nb + 2 * kT - 1) / (2 * kT))), kT, 0, s>>>(
       C, S, nb, c->hii, ta.s_off, ta.s_idx, ta.s_info, c->jb);
-  crt_add_kernel<<<grid_of(N), kT, 0, s>>>(c->oz.prod, na, nb, c->oz.h0e[0], c->oz.cte, S);
+  crt_add_kernel<<<(unsigned)na, kT, 0, s>>>(c->oz.prod, na, nb, c->oz.h0e[0], c->oz.cte, S);
   SBD_CUDA(cudaGetLastError());
   if (events) SBD_CUDA(cudaEventRecord(c->ev[1], s));
   // beta: sigma^T = H0b (C^T), with H0b's rows and C's rows scaled
@@ -311,8 +386,8 @@ bool same_spin_ozaki_fp64(sbdgpu_ctx* c, const double* C, double* S, double* ct,
     if (!gemm_i8(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)nb, (int)na, (int)nb, c->oz.h0r[1] + (size_t)l * nb * nb, (int)nb,
                  c->oz.cr + (size_t)l * N, (int)nb, c->oz.prod + (size_t)l * N, (int)nb))
       throw Error{SBDGPU_ERR_CUDA, "INT8 product refused after the alpha products ran"};
-  crt_add_kernel<<<grid_of(N), kT, 0, s>>>(c->oz.prod, na, nb, c->oz.ce, c->oz.h0e[1], S);
-  jsingles64_kernel<false><<<dim3((unsigned)nb, (unsigned)((na + kT - 1) / kT)), kT, 0, s>>>(
+  crt_add_kernel<<<(unsigned)na, kT, 0, s>>>(c->oz.prod, na, nb, c->oz.ce, c->oz.h0e[1], S);
+  jsingles64_kernel<false><<<dim3((unsigned)nb, (unsigned)((na + 2 * kT - 1) / (2 * kT))), kT, 0, s>>>(
       ct, st, na, nullptr, tb.s_off, tb.s_idx, tb.s_info, c->ja);
   SBD_CUDA(cudaGetLastError());
   transpose_add(st, S, nb, na, s);
