@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "internal.cuh"
 
@@ -73,25 +74,63 @@ __global__ void absmax_kernel(const float* __restrict__ x, size_t n, unsigned in
   if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as integers
 }
 
-// S[row - row0][col] (=) [hii * C] + sum over the bra's singles of s J_pq[col] C[ket][col]
-template <bool kWithDiag>
+// S[row][col] (=) [hii * C] + sum over the bra's singles of s J_pq[col] C[ket][col];
+// V consecutive columns per thread (V = 4: ncols a multiple of 4 and the
+// arrays 16-byte aligned)
+template <bool kWithDiag, int V>
 __global__ void __launch_bounds__(kJThreads) jsingles_kernel(const float* __restrict__ C, float* __restrict__ S,
                                                              size_t ncols, const double* __restrict__ hii,
                                                              const int64_t* __restrict__ s_off,
                                                              const int32_t* __restrict__ s_idx,
                                                              const uint32_t* __restrict__ s_info,
                                                              const float* __restrict__ J) {
+  using Vec = typename std::conditional<V == 4, float4, float>::type;
   const size_t row = blockIdx.x;
-  const size_t col = (size_t)blockIdx.y * kJThreads + threadIdx.x;
+  const size_t col = V * ((size_t)blockIdx.y * kJThreads + threadIdx.x);
   if (col >= ncols) return;
-  float acc = kWithDiag ? (float)hii[row * ncols + col] * C[row * ncols + col] : 0.f;
-  for (int64_t k = s_off[row]; k < s_off[row + 1]; k++) {
+  float acc[V];
+#pragma unroll
+  for (int v = 0; v < V; v++) acc[v] = 0.f;
+  if (kWithDiag) {
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v] = (float)hii[row * ncols + col + v] * C[row * ncols + col + v];
+  }
+  const int64_t k1 = s_off[row + 1];
+#pragma unroll 4
+  for (int64_t k = s_off[row]; k < k1; k++) {
     const size_t j = (size_t)__ldg(&s_idx[k]);
     const uint32_t info = __ldg(&s_info[k]);
-    const float jv = __ldg(&J[(size_t)((info >> 12) & 0xFFFu) * ncols + col]);
-    acc += ((info & 0x80000000u) ? -jv : jv) * __ldg(&C[j * ncols + col]);
+    const Vec jv = __ldg(reinterpret_cast<const Vec*>(J + (size_t)((info >> 12) & 0xFFFu) * ncols + col));
+    const Vec x = __ldg(reinterpret_cast<const Vec*>(C + j * ncols + col));
+    const float sg = (info & 0x80000000u) ? -1.f : 1.f;
+    const float* jp = reinterpret_cast<const float*>(&jv);
+    const float* xp = reinterpret_cast<const float*>(&x);
+#pragma unroll
+    for (int v = 0; v < V; v++) acc[v] = fmaf(sg * jp[v], xp[v], acc[v]);
   }
-  S[row * ncols + col] = acc;
+  if constexpr (V == 4) {
+    *reinterpret_cast<float4*>(S + row * ncols + col) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+  } else {
+    S[row * ncols + col] = acc[0];
+  }
+}
+
+// one jsingles pass over rows x ncols, four columns per thread where the
+// shapes and pointers allow
+template <bool kWithDiag>
+void launch_jsingles(const float* C, float* S, size_t rows, size_t ncols, const double* hii, const SpinTables& t,
+                     const float* J, cudaStream_t s) {
+  const bool vec4 = ncols % 4 == 0 && (((uintptr_t)C | (uintptr_t)S | (uintptr_t)J) & 15) == 0;
+  if (vec4) {
+    const unsigned gy = (unsigned)((ncols / 4 + kJThreads - 1) / kJThreads);
+    jsingles_kernel<kWithDiag, 4><<<dim3((unsigned)rows, gy), kJThreads, 0, s>>>(C, S, ncols, hii, t.s_off, t.s_idx,
+                                                                                 t.s_info, J);
+  } else {
+    const unsigned gy = (unsigned)((ncols + kJThreads - 1) / kJThreads);
+    jsingles_kernel<kWithDiag, 1><<<dim3((unsigned)rows, gy), kJThreads, 0, s>>>(C, S, ncols, hii, t.s_off, t.s_idx,
+                                                                                 t.s_info, J);
+  }
+  SBD_CUDA(cudaGetLastError());
 }
 
 constexpr float kHScale = 256.f;  // the string-only elements are O(1): 2^8 keeps their lo parts normal in FP16
@@ -166,9 +205,7 @@ void same_spin_dense_fp32(sbdgpu_ctx* c, const float* C, float* S, float* ct, fl
   const size_t na = c->na, nb = c->nb;
   if (events) SBD_CUDA(cudaEventRecord(c->ev[0], s));
   // diagonal and the alpha singles' J part
-  jsingles_kernel<true><<<dim3((unsigned)na, (unsigned)((nb + kJThreads - 1) / kJThreads)), kJThreads, 0, s>>>(
-      C, S, nb, c->hii, ta.s_off, ta.s_idx, ta.s_info, c->jb32);
-  SBD_CUDA(cudaGetLastError());
+  launch_jsingles<true>(C, S, na, nb, c->hii, ta, c->jb32, s);
   // C split into FP16 hi + lo, scaled by a power of two that puts max|C| near 2^14
   unsigned int* amax = reinterpret_cast<unsigned int*>(c->red);
   SBD_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned int), s));
@@ -204,9 +241,7 @@ void same_spin_dense_fp32(sbdgpu_ctx* c, const float* C, float* S, float* ct, fl
                           yb[k], CUDA_R_16F, (int)nb, &one, S, CUDA_R_32F, (int)nb, CUBLAS_COMPUTE_32F,
                           CUBLAS_GEMM_DEFAULT));
   transpose(C, ct, na, nb, s);
-  jsingles_kernel<false><<<dim3((unsigned)nb, (unsigned)((na + kJThreads - 1) / kJThreads)), kJThreads, 0, s>>>(
-      ct, st, na, nullptr, tb.s_off, tb.s_idx, tb.s_info, c->ja32);
-  SBD_CUDA(cudaGetLastError());
+  launch_jsingles<false>(ct, st, nb, na, nullptr, tb, c->ja32, s);
   transpose_add(st, S, nb, na, s);
   if (events) SBD_CUDA(cudaEventRecord(c->ev[2], s));
 }
