@@ -318,6 +318,14 @@ def time_to_e0(ctx, args, learned=None):
                               "within_1e-6": abs(e_l - e_ref) < 1e-6, "final_residual": float(ttl[-1]),
                               "speedup_vs_plain": t_plain / t_l, "speedup_vs_mixed_diagonal": t_mp / t_l,
                               "network": info}
+        if args.olsen:
+            t = time.perf_counter()
+            e_o, _, to_, tto = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED, restart_keep=3,
+                                            restart_prev=1, precond=sbd_b200.PRECOND_OLSEN)
+            t_o = time.perf_counter() - t
+            out["olsen"] = {"steps": len(to_), "s": t_o, "e": e_o, "abs_err": abs(e_o - e_ref),
+                            "within_1e-6": abs(e_o - e_ref) < 1e-6, "final_residual": float(tto[-1]),
+                            "speedup_vs_plain": t_plain / t_o, "speedup_vs_mixed_diagonal": t_mp / t_o}
         return out
     t = time.perf_counter()
     e_mix, _, tm, ttm = ctx.davidson(W0, 100, 10, args.mixed_tol, precision=sbd_b200.MIXED)
@@ -775,6 +783,7 @@ def main():
     ap.add_argument("--roots", type=int, default=0, help="also time block Davidson for this many roots")
     ap.add_argument("--roots-workload", default="c1_L26_6e_4000", help="workload of the block Davidson block")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner run")
+    ap.add_argument("--olsen", action="store_true", help="also time the mixed run with Olsen's correction")
     ap.add_argument("--learn-pairs", type=int, default=12, help="harvested triples for the learned preconditioner")
     ap.add_argument("--learn-cg", type=int, default=40, help="MINRES steps per harvested correction")
     ap.add_argument("--learn-steps", type=int, default=600, help="Adam steps of the learned preconditioner")

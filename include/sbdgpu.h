@@ -67,7 +67,7 @@ typedef struct sbdgpu_opts {
                        vector at a restart (the "+1" of a GD+k restart), with its
                        sigma vector; 0 = not (the reference's behaviour) */
   int precond;      /* mixed precisions only: SBDGPU_PRECOND_DIAGONAL (the reference's
-                       correction) or SBDGPU_PRECOND_LEARNED */
+                       correction), SBDGPU_PRECOND_LEARNED or SBDGPU_PRECOND_OLSEN */
 } sbdgpu_opts;
 
 /* Davidson correction (sbdgpu_opts.precond). */
@@ -78,6 +78,10 @@ typedef struct sbdgpu_opts {
                                      correction when the context has no network, or
                                      for the rest of the run after a restart cycle in
                                      which the residual norm fell by less than 10 % */
+#define SBDGPU_PRECOND_OLSEN 2    /* t = P r - eps P w, P = (E0 - H_ii)^-1 regularised as
+                                     the diagonal correction, w the Ritz vector and
+                                     eps = <w|P r> / <w|P w> (Olsen's correction; no
+                                     counterpart in the reference) */
 
 /* Training of the learned preconditioner (no counterpart in the reference). */
 typedef struct sbdgpu_learn_opts {

@@ -37,6 +37,7 @@ EXPORTS = [
 
 PRECOND_DIAGONAL = 0
 PRECOND_LEARNED = 1
+PRECOND_OLSEN = 2
 
 
 class SbdGpuError(RuntimeError):

@@ -216,6 +216,18 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
     HC[k] = (float*)sbdgpu::dev_alloc(sizeof(float) * n);
   }
   X = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
+  // Olsen's correction needs P applied to the Ritz vector as well
+  const bool olsen = o->precond == SBDGPU_PRECOND_OLSEN;
+  double* Y = nullptr;
+  struct FreeY {
+    double** y;
+    cudaStream_t s;
+    ~FreeY() {
+      cudaStreamSynchronize(s);
+      cudaFree(*y);
+    }
+  } guard_y{&Y, st};
+  if (olsen) Y = (double*)sbdgpu::dev_alloc(sizeof(double) * n);
   const double eps_reg = 1.0e-12;
   std::vector<double> H(nb * nb, 0.0), U(nb * nb, 0.0), E(nb, 0.0);
   std::vector<double> step_times;
@@ -257,10 +269,19 @@ void davidson_mixed(sbdgpu_ctx* c, const sbdgpu_opts* o, double* W, double* R, d
   double tol_learned_cycle = 1e300;
   double tol_thick_cycle = 1e300;
   auto add_correction = [&](int into, double e0) {
-    if (use_learned)
+    if (use_learned) {
       sbdgpu::learned_precondition(c, R, e0, eps_reg, X);
-    else
+    } else {
       sbdgpu::precondition(R, c->hii, e0, eps_reg, X, n, st);
+      if (olsen) {
+        // t = P r - eps P w with eps = <w|P r> / <w|P w>: the correction is
+        // P-orthogonal to the Ritz vector w, so it does not fall back onto w
+        // where P r is nearly parallel to it
+        sbdgpu::precondition(W, c->hii, e0, eps_reg, Y, n, st);
+        const double wpw = sbdgpu::dot(c, W, Y, n);
+        if (std::fabs(wpw) > 0.0) sbdgpu::axpy(X, Y, -sbdgpu::dot(c, W, X, n) / wpw, n, st);
+      }
+    }
     for (int pass = 0; pass < gs_passes; pass++)
       for (int kb = 0; kb < into; kb++) {
         double olap = sbdgpu::dot_f(c, C[kb], X, C[kb], n);  // <X|C_kb> with X in FP64
@@ -571,7 +592,8 @@ int sbdgpu_davidson(sbdgpu_ctx* c, const sbdgpu_opts* o, double* Wh, double* ene
   return guarded(c, [&] {
     if (!o || !Wh) throw Error{SBDGPU_ERR_ARG, "null argument"};
     check_precision(o->precision);
-    if (o->precond != SBDGPU_PRECOND_DIAGONAL && o->precond != SBDGPU_PRECOND_LEARNED)
+    if (o->precond != SBDGPU_PRECOND_DIAGONAL && o->precond != SBDGPU_PRECOND_LEARNED &&
+        o->precond != SBDGPU_PRECOND_OLSEN)
       throw Error{SBDGPU_ERR_ARG, "unsupported precond " + std::to_string(o->precond)};
     int nb = o->max_nb;
     if (nb < 1 || nb > 32) throw Error{SBDGPU_ERR_ARG, "max_nb must be in [1, 32]"};

@@ -33,6 +33,24 @@ def test_mixed_davidson_energy(golden):
     assert abs(abs(np.dot(W, golden["W"])) - 1.0) < 1e-6
 
 
+def test_mixed_davidson_olsen_correction(golden):
+    """Olsen's correction (the diagonal correction made P-orthogonal to the
+    Ritz vector) reaches the reference's energy with the thick restart; an
+    unknown correction is refused."""
+    if "energy" not in golden:
+        pytest.skip("fixture has no Davidson result")
+    ctx = gpu_ctx(golden)
+    W0 = np.zeros(ctx.n)
+    W0[0] = 1.0
+    e, W, te, tt = ctx.davidson(W0, 1000, 10, 1e-5, precision=sbd_b200.MIXED, restart_keep=3, restart_prev=1,
+                                precond=sbd_b200.PRECOND_OLSEN)
+    assert abs(e - float(golden["energy"])) < 1e-6
+    assert tt[-1] < 1e-5
+    assert abs(abs(np.dot(W, golden["W"])) - 1.0) < 1e-6
+    with pytest.raises(sbd_b200.SbdGpuError):
+        ctx.davidson(W0, 10, 10, 1e-5, precision=sbd_b200.MIXED, precond=3)
+
+
 def test_mixed_thick_restart(golden):
     """Thick restart (the 3 lowest Ritz vectors and their sigma kept) reaches the
     same energy in no more sigma builds than the reference's collapse restart."""
