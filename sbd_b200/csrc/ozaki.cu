@@ -36,7 +36,7 @@ namespace {
 
 constexpr int kMods = 15;
 constexpr int kBits = 49;
-constexpr int kMaxExp = 1000;  // 2^kMaxExp and 2^-(kMaxExp - kBits) are normal doubles
+constexpr int kMaxExp = 1000;  // scale exponents lie in [kBits - 1024, kMaxExp]: 2^e is a normal double
 constexpr int kT = 256;
 
 // the primes, as compile-time constants wherever the index is one (the
