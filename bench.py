@@ -132,7 +132,40 @@ def table_stats(ctx):
     for spin in (0, 1):
         so, si, do, di = ctx.tables(spin)
         st[spin] = (len(si), len(di))
+        st[("singles", spin)] = np.diff(so.astype(np.int64))
     return st
+
+
+def ab_smem_floor(st, group, sm_count, sm_mhz):
+    """The shared-memory wavefront floor of the FP64 alpha-beta kernel
+    (csrc/sigma.cu ab_kernel): every CTA (one source alpha string, `group` of
+    its singles) walks every 32-string slice of beta strings for as many steps
+    as the slice's longest singles list; a step is group/2 128-bit integral
+    loads of 32 distinct rows (4 wavefronts each) and one 64-bit gather of C
+    (2 wavefronts); an SM retires one wavefront per cycle.  Lanes of a warp
+    that read the same integral row take fewer wavefronts, so the measured time
+    can sit slightly below this figure."""
+    na_s = st[("singles", 0)]
+    nb_s = st[("singles", 1)]
+    ctas = int(np.sum((na_s + group - 1) // group))
+    pad = (-len(nb_s)) % 32
+    widths = np.concatenate([nb_s, np.zeros(pad, np.int64)]).reshape(-1, 32).max(axis=1)
+    warp_steps = ctas * int(widths.sum())
+    per_step = 4 * (group // 2) + 2
+    floor_ms = warp_steps * per_step / sm_count / (sm_mhz * 1e3)
+    return {"group": group, "wavefronts_per_step": per_step, "ctas": ctas, "warp_steps": warp_steps,
+            "sm_count": sm_count, "sm_mhz": sm_mhz, "floor_ms": floor_ms}
+
+
+def ab_default_group(nb, P, smem_optin):
+    """The FP64 alpha-beta group size the library picks without a tuning table:
+    the largest of 16, 8, 4, 2 whose integral rows ([P][group + 2] doubles) fit
+    in shared memory next to one row of C (csrc/sigma.cu alpha_beta)."""
+    crow = (nb * 8 + 15) // 16 * 16
+    for g in (16, 8, 4, 2):
+        if crow + P * (g + 2) * 8 <= smem_optin - 1024:
+            return g
+    return None
 
 
 def algorithmic(ctx, st):
@@ -704,6 +737,16 @@ def run_gpu(args):
     traffic = args.traffic
     if traffic is None and dom == 2:
         traffic = AB_TRAFFIC_BYTES_PER_DET * n
+    smem_floor = None
+    if dom == 2:
+        props = torch.cuda.get_device_properties(dev)
+        group = ab_default_group(ctx.nb, ctx.norb * (ctx.norb + 1) // 2,
+                                 getattr(props, "shared_memory_per_block_optin", 232448))
+        clk = sampler.summary().get("sm_mhz") or 1965.0
+        if group:
+            smem_floor = ab_smem_floor(st, group, props.multi_processor_count, clk)
+            smem_floor["measured_ms"] = ab_ms
+            smem_floor["frac"] = smem_floor["floor_ms"] / ab_ms
     line = {
         "metric": METRIC, "value": world * 1000.0 / t_step, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
@@ -720,7 +763,8 @@ def run_gpu(args):
                      "traffic": traffic,
                      "limiter": ("shared-memory pipe: one gathered 8-byte integral per FP64 FMA (ncu at 16M "
                                  "dets: l1tex 90.8 %, FP64 pipe 24.7 %, profiles/ab_kernel_c1_L26_6e_4000.md)")
-                     if dom == 2 else "L1/L2 streaming of C rows (profiles/rows_kernel_c1_L26_6e_4000.md)"},
+                     if dom == 2 else "L1/L2 streaming of C rows (profiles/rows_kernel_c1_L26_6e_4000.md)",
+                     "smem_floor": smem_floor},
         "phases_ms": {"alpha_same_spin_with_diag": parts[0] / args.steps,
                       "beta_same_spin": parts[1] / args.steps, "alpha_beta": ab_ms},
         "flops_per_sigma": alg["flops"], "fp64_tflops": alg["flops"] / (t_step * 1e-3) / 1e12,
