@@ -216,7 +216,9 @@ void same_spin_dense_fp32(sbdgpu_ctx* c, const float* C, float* S, float* ct, fl
   SBD_CUDA(cudaStreamSynchronize(s));
   float cmax = 0.f;
   std::memcpy(&cmax, &bits, sizeof(float));
-  const float cscale = cmax > 0.f ? std::ldexp(1.0f, 14 - (int)std::ceil(std::log2(cmax))) : 1.0f;
+  // a NaN or an infinity in C keeps the scale at 1 and reaches sigma through the products
+  const float cscale =
+      cmax > 0.f && std::isfinite(cmax) ? std::ldexp(1.0f, 14 - (int)std::ceil(std::log2(cmax))) : 1.0f;
   __half* chi = static_cast<__half*>(c->c16[0]);
   __half* clo = static_cast<__half*>(c->c16[1]);
   split_fp16_kernel<<<592, 256, 0, s>>>(C, c->N, cscale, chi, clo);

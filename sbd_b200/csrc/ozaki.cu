@@ -38,6 +38,7 @@ constexpr int kMods = 15;
 constexpr int kBits = 49;
 constexpr int kMaxExp = 1000;  // scale exponents lie in [kBits - 1024, kMaxExp]: 2^e is a normal double
 constexpr int kT = 256;
+constexpr int kNonFinite = 0x40000000;  // row exponent of a row holding a NaN or an infinity
 
 // the primes, as compile-time constants wherever the index is one (the
 // compiler then reduces by multiply-high and shift, not by a division)
@@ -75,18 +76,33 @@ __device__ __forceinline__ int scale_exp(double amax) {
   return min(kBits - ex, kMaxExp);
 }
 
-// per-row exponent of a row-major [rows][cols] matrix
+// per-row exponent of a row-major [rows][cols] matrix; kNonFinite for a row
+// holding a NaN or an infinity (the product then carries a NaN into every
+// entry that row feeds, as the FP64 product would carry it)
 __global__ void __launch_bounds__(kT) row_exp_kernel(const double* __restrict__ X, size_t cols, int* __restrict__ e) {
   __shared__ double sh[kT / 32];
+  __shared__ int bad_sh[kT / 32];
   const size_t r = blockIdx.x;
   double m = 0.0;
-  for (size_t c = threadIdx.x; c < cols; c += kT) m = fmax(m, fabs(X[r * cols + c]));
+  bool bad = false;
+  for (size_t c = threadIdx.x; c < cols; c += kT) {
+    const double x = X[r * cols + c];
+    bad |= !isfinite(x);
+    m = fmax(m, fabs(x));
+  }
   for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  bad = __any_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0) {
+    sh[threadIdx.x >> 5] = m;
+    bad_sh[threadIdx.x >> 5] = bad;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < kT / 32; w++) m = fmax(m, sh[w]);
-    e[r] = scale_exp(fmax(m, sh[0]));
+    for (int w = 1; w < kT / 32; w++) {
+      m = fmax(m, sh[w]);
+      bad |= bad_sh[w] != 0;
+    }
+    e[r] = bad ? kNonFinite : scale_exp(fmax(m, sh[0]));
   }
 }
 
@@ -120,12 +136,21 @@ __device__ __forceinline__ void store_all_residues(std::index_sequence<L...>, co
 __global__ void __launch_bounds__(kT) residue_kernel(const double* __restrict__ X, size_t rows, size_t cols,
                                                     const int* __restrict__ e, int8_t* __restrict__ out) {
   const size_t n = rows * cols, row = blockIdx.x;
-  const double scale = pow2(e[row]);  // e <= kMaxExp; >= kBits - 1024
+  const int er = e[row];
+  const double scale = er == kNonFinite ? 0.0 : pow2(er);  // e <= kMaxExp; >= kBits - 1024
   const double* xr = X + row * cols;
   for (size_t c = 4 * (size_t)threadIdx.x; c < cols; c += 4 * kT) {
-    const double2 x01 = *reinterpret_cast<const double2*>(xr + c);
-    const double2 x23 = *reinterpret_cast<const double2*>(xr + c + 2);
-    const double x[4] = {x01.x, x01.y, x23.x, x23.y};
+    double x[4];
+    if (er == kNonFinite) {
+      x[0] = x[1] = x[2] = x[3] = 0.0;  // residues 0: the reconstruction writes NaN for this row
+    } else {
+      const double2 x01 = *reinterpret_cast<const double2*>(xr + c);
+      const double2 x23 = *reinterpret_cast<const double2*>(xr + c + 2);
+      x[0] = x01.x;
+      x[1] = x01.y;
+      x[2] = x23.x;
+      x[3] = x23.y;
+    }
     unsigned hu[4], lo[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -185,7 +210,12 @@ __global__ void __launch_bounds__(kT) crt_add_kernel(const int32_t* __restrict__
     unsigned __int128 x = acc - qm;
     while (x >= M) x -= M;
     const double v = x > (M >> 1) ? -u128_to_double(M - x) : u128_to_double(x);  // the symmetric representative
-    const int s = -(er + e_col[c]);
+    const int ec = e_col[c];
+    if (er == kNonFinite || ec == kNonFinite) {
+      S[i] = __longlong_as_double(0x7FF8000000000000LL);  // NaN
+      continue;
+    }
+    const int s = -(er + ec);
     S[i] += (s >= -1022 && s <= 1023) ? v * pow2(s) : ldexp(v, s);
   }
 }

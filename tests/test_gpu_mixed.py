@@ -100,6 +100,33 @@ def test_mixed_sigma_dense_same_spin(norb, ne, count, seed):
     assert tt[-1] < 1e-4 and abs(e32 - e64) < 1e-6
 
 
+def test_fp64_same_spin_integer_products_non_finite_input():
+    """A NaN or an infinity in C makes sigma non-finite wherever the rows
+    kernels make it non-finite (the integer products mark the whole row or
+    column they feed), and leaves the finite entries as they were."""
+    import sbd_b200
+    from sbd_b200 import synth
+    from conftest import seeded_vector
+    ints, ne, strs = synth.make_small(16, 5, 1100, 33)
+    ctx = sbd_b200.context_from_integrals(ints, strs, strs)
+    C = seeded_vector(ctx.n, 33)
+    C[5 * ctx.nb + 17] = np.nan
+    C[700 * ctx.nb + 3] = np.inf
+    ctx.set_fp64_same_spin(1)
+    ref = ctx.sigma(C)
+    ctx.set_fp64_same_spin(0)
+    got = ctx.sigma(C)
+    bad_ref, bad_got = ~np.isfinite(ref), ~np.isfinite(got)
+    assert bad_ref.any() and np.all(bad_got[bad_ref])
+    both = ~bad_ref & ~bad_got
+    assert both.sum() > ctx.n // 2
+    assert np.abs(got[both] - ref[both]).max() <= 1e-12 * np.abs(ref[both]).max()
+    # the mixed sigma (split-FP16 same-spin products) carries them as well
+    mixed = ctx.sigma(C, precision=sbd_b200.MIXED)
+    assert np.all(~np.isfinite(mixed)[bad_ref])
+    ctx.close()
+
+
 @pytest.mark.parametrize("norb,ne,count,seed", [(16, 5, 1100, 31), (18, 4, 1500, 32), (16, 5, 1102, 33)])
 def test_fp64_same_spin_integer_products(norb, ne, count, seed):
     """From 1,024 strings per spin (multiples of 4) the FP64 sigma forms its
