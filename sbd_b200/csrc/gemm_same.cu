@@ -167,10 +167,12 @@ bool ensure_dense_same(sbdgpu_ctx* c) {
   }
   cudaFree(tmp);
   for (int part = 0; part < 2; part++) c->c16[part] = dev_alloc(sizeof(__half) * c->N);
-  cublasHandle_t h = nullptr;
-  SBD_BLAS(cublasCreate(&h));
-  c->blas = h;
-  SBD_BLAS(cublasSetStream(h, c->stream));
+  if (!c->blas) {  // the INT8 same-spin products may have made the context's handle already
+    cublasHandle_t h = nullptr;
+    SBD_BLAS(cublasCreate(&h));
+    c->blas = h;
+  }
+  SBD_BLAS(cublasSetStream(static_cast<cublasHandle_t>(c->blas), c->stream));
   return true;
 }
 

@@ -334,18 +334,24 @@ bool ensure_ozaki(sbdgpu_ctx* c) {
     }
   } catch (...) {
     cudaFree(tmp);
+    free_ozaki(c);
     throw;
   }
   cudaFree(tmp);
-  c->oz.cr = (int8_t*)dev_alloc((size_t)kMods * N);
-  c->oz.ctr = (int8_t*)dev_alloc((size_t)kMods * N);
-  c->oz.ce = (int*)dev_alloc(sizeof(int) * na);
-  c->oz.cte = (int*)dev_alloc(sizeof(int) * nb);
-  c->oz.prod = (int32_t*)dev_alloc(sizeof(int32_t) * (size_t)kMods * N);
-  if (!c->blas) {
-    cublasHandle_t h = nullptr;
-    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) throw Error{SBDGPU_ERR_CUDA, "cublasCreate failed"};
-    c->blas = h;
+  try {
+    c->oz.cr = (int8_t*)dev_alloc((size_t)kMods * N);
+    c->oz.ctr = (int8_t*)dev_alloc((size_t)kMods * N);
+    c->oz.ce = (int*)dev_alloc(sizeof(int) * na);
+    c->oz.cte = (int*)dev_alloc(sizeof(int) * nb);
+    c->oz.prod = (int32_t*)dev_alloc(sizeof(int32_t) * (size_t)kMods * N);
+    if (!c->blas) {
+      cublasHandle_t h = nullptr;
+      if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) throw Error{SBDGPU_ERR_CUDA, "cublasCreate failed"};
+      c->blas = h;
+    }
+  } catch (...) {
+    free_ozaki(c);  // nothing half-built stays behind for a later call to overwrite
+    throw;
   }
   cublasSetStream(static_cast<cublasHandle_t>(c->blas), st);
   c->oz.ready = true;
