@@ -107,7 +107,9 @@ template <int NW>
 __device__ __forceinline__ int64_t find_state(const uint64_t* __restrict__ hkeys, const int64_t* __restrict__ hidx,
                                               uint64_t hmask, const uint64_t* w) {
   uint64_t h = hash_state<NW>(w) & hmask;
-  for (;;) {  // the table is at most half full, so an empty slot ends every probe sequence
+  // the table is at most half full, so an empty slot ends every probe
+  // sequence; the bound keeps the loop finite regardless
+  for (uint64_t probe = 0; probe <= hmask; probe++) {
     const int64_t id = __ldg(&hidx[h]);
     if (id < 0) return -1;
     bool eq = true;
@@ -116,6 +118,7 @@ __device__ __forceinline__ int64_t find_state(const uint64_t* __restrict__ hkeys
     if (eq) return id;
     h = (h + 1) & hmask;
   }
+  return -1;
 }
 
 // parity of the occupied sites below q
