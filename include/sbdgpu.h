@@ -301,7 +301,8 @@ int sbdgpu_autotune(sbdgpu_ctx* ctx, int reps, int* ab_group, int* ab_threads, f
  * operator (residues modulo 15 primes, CRT reconstruction; FP64-accurate: the
  * scaled operands are rounded to 49-bit integers) where both spins have at
  * least 1,024 strings (multiples of 4) and the residues fit in device memory,
- * else the rows kernels; method 1 = the rows kernels always. */
+ * else the rows kernels; method 1 = the rows kernels always (and the device
+ * memory of the integer products is released). */
 int sbdgpu_set_fp64_same_spin(sbdgpu_ctx* ctx, int method);
 
 const char* sbdgpu_last_error(sbdgpu_ctx* ctx);

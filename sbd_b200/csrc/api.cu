@@ -783,6 +783,7 @@ int sbdgpu_set_fp64_same_spin(sbdgpu_ctx* c, int method) {
     if (method != 0 && method != 1) throw Error{SBDGPU_ERR_ARG, "method must be 0 or 1"};
     SBD_CUDA(cudaStreamSynchronize(c->stream));
     c->oz.mode = method;
+    if (method == 1) sbdgpu::free_ozaki(c);  // the residues of the operators go back to the device
   });
 }
 

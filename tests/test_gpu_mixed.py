@@ -145,7 +145,11 @@ def test_fp64_same_spin_integer_products(norb, ne, count, seed):
     got = ctx.sigma(C)
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
     C2 = C * np.exp(np.random.default_rng(seed).normal(size=ctx.n) * 4)  # wide dynamic range
-    ctx.set_fp64_same_spin(1)
+    import torch
+    free0 = torch.cuda.mem_get_info(0)[0]
+    ctx.set_fp64_same_spin(1)  # releases the integer products' buffers (re-made below)
+    if count % 4 == 0:
+        assert torch.cuda.mem_get_info(0)[0] - free0 >= 15 * (ctx.na ** 2 + ctx.nb ** 2)
     ref2 = ctx.sigma(C2)
     ctx.set_fp64_same_spin(0)
     got2 = ctx.sigma(C2)
